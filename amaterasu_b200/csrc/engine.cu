@@ -1,0 +1,963 @@
+// The H.psi engine: sphere<->grid maps, the three fused FFT stages, the nonlocal
+// projector products and the density accumulation.
+//
+// Layout in HBM
+//   psi, hpsi      per k-point a row-major (nbands, npw_k) block, blocks back to back.
+//   work           per band the x-planes that can hold sphere coefficients ("slots",
+//                  2*h_max+1 of the n1 planes), each a full (n2, n3) plane:
+//                  work[band][slot][y][z]. After stage A the plane is in real space along
+//                  y and z, after stage B also along x and already multiplied by V.
+//   V              per spin, real, in the permuted real-space order the in-place DFTs
+//                  produce (see dft.cuh), pre-scaled by 1/N (the forward-transform norm).
+//
+// Stage A  (grid: slot x band)   scatter the slot's sphere points into a zeroed smem plane,
+//                                backward DFT along z (only rows holding points), then y.
+// Stage B  (grid: y x band)      gather the slots' rows at one y into an (n1, n3) smem slab,
+//                                backward DFT along x, multiply by V, forward DFT along x,
+//                                write the slot rows back.
+// Stage C  (grid: slot x band)   forward DFT along y, then z (rows holding points), gather
+//                                the sphere points and write T*psi + that into hpsi.
+// The nonlocal term is added by two GEMMs: P = psi B^H (split-K), hpsi += P (D B).
+#include "common.cuh"
+#include "dft.cuh"
+#include "gemm.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <numeric>
+#include <vector>
+
+namespace ama {
+
+struct AxisPlan { int n, A, B; };
+
+static bool split_length(int n, AxisPlan* out) {
+  // n = A*B with A, B in the codelet set; minimise max(A, B), prefer A >= B.
+  auto ok = [](int r) { return r >= 1 && r <= 16 && r != 13; };
+  int best_a = -1, best_b = -1;
+  for (int b = 1; b <= 16; ++b) {
+    if (n % b) continue;
+    int a = n / b;
+    if (!ok(a) || !ok(b) || a < b) continue;
+    if (best_a < 0 || std::max(a, b) < std::max(best_a, best_b)) { best_a = a; best_b = b; }
+  }
+  if (best_a < 0) return false;
+  *out = {n, best_a, best_b};
+  return true;
+}
+
+
+struct DeviceTables {
+  int* plane_x = nullptr;      // [nslots]
+  int* slot_of_x = nullptr;    // [n1] -> slot or -1
+  int2* entries = nullptr;     // [sum npw]: (g, y*n3+z) grouped by (k, slot)
+  int* entry_start = nullptr;  // [nk*(nslots+1)]
+  int* rows = nullptr;         // concatenated y rows per (k, slot)
+  int* row_start = nullptr;    // [nk*(nslots+1)]
+  int64_t* pw_off = nullptr;   // [nk+1]
+  int* npw = nullptr;          // [nk]
+  double* kin64 = nullptr;     // [sum npw]
+  float* kin32 = nullptr;
+  void* tw[2][3][2] = {};      // [prec][axis][0 backward,1 forward]
+  void* proj[2] = {};          // [prec] B, k-major (nproj, npw_k) blocks
+  void* dproj[2] = {};         // [prec] D.B
+  double* v64 = nullptr;       // [nspin][N] permuted, /N
+  float* v32 = nullptr;
+};
+
+}  // namespace ama
+
+using namespace ama;
+
+struct AmaEngine {
+  AxisPlan ax[3];
+  int64_t N = 0;
+  int nk = 0, nspin = 1, nproj = 0, nslots = 0;
+  uint32_t precisions = 0;
+  std::vector<int> npw;
+  std::vector<int64_t> pw_off;
+  int max_npw = 0;
+  int max_rows = 0;
+  DeviceTables d;
+  bool has_potential = false;
+  // workspaces (grown on demand)
+  void* work[2] = {};
+  size_t work_bytes[2] = {};
+  void* ws_proj[2] = {};       // P = psi B^H
+  size_t ws_proj_bytes[2] = {};
+  void* ws_part[2] = {};       // split-K partials
+  size_t ws_part_bytes[2] = {};
+  double* ws_dens = nullptr;   // permuted density accumulator
+  size_t ws_dens_bytes = 0;
+};
+
+namespace {
+
+template <typename T> cudaError_t grow(void** ptr, size_t* have, size_t need) {
+  if (*have >= need) return cudaSuccess;
+  if (*ptr) cudaFree(*ptr);
+  *ptr = nullptr;
+  *have = 0;
+  cudaError_t e = cudaMalloc(ptr, need);
+  if (e == cudaSuccess) *have = need;
+  return e;
+}
+
+template <typename T> int upload(T** dst, const T* src, size_t count) {
+  AMA_CUDA_TRY(cudaMalloc((void**)dst, std::max<size_t>(count, 1) * sizeof(T)));
+  if (count) AMA_CUDA_TRY(cudaMemcpy(*dst, src, count * sizeof(T), cudaMemcpyHostToDevice));
+  return AMA_OK;
+}
+
+// ------------------------------------------------------------------ kernels
+struct HpsiView {
+  int n1, n2, n3;
+  int A1, B1, A2, B2, A3, B3;
+  int nslots;
+  const int* plane_x;
+  const int* slot_of_x;
+  const int2* entries;
+  const int* entry_start;
+  const int* rows;
+  const int* row_start;
+  const int64_t* pw_off;
+  const int* npw;
+  int k_first, nbands;
+  int64_t plane_elems, band_elems;  // n2*n3, nslots*n2*n3
+};
+
+template <typename C>
+__device__ __forceinline__ void load_twiddles(C* dst, const C* src, int n) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+}
+
+template <typename T>
+__global__ void stage_a_kernel(HpsiView v, const cx_t<T>* __restrict__ tw_y,
+                               const cx_t<T>* __restrict__ tw_z,
+                               const cx_t<T>* __restrict__ psi, cx_t<T>* __restrict__ work) {
+  using C = cx_t<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* plane = reinterpret_cast<C*>(smem_raw);
+  C* sty = plane + v.plane_elems;
+  C* stz = sty + v.n2;
+  int* rows = reinterpret_cast<int*>(stz + v.n3);
+
+  const int slot = blockIdx.x;
+  const int gb = blockIdx.y;
+  const int kl = gb / v.nbands, band = gb % v.nbands;
+  const int k = v.k_first + kl;
+  const int npw = v.npw[k];
+  const C* src = psi + (v.pw_off[k] - v.pw_off[v.k_first]) * v.nbands + (int64_t)band * npw;
+
+  load_twiddles(sty, tw_y, v.n2);
+  load_twiddles(stz, tw_z, v.n3);
+  for (int64_t i = threadIdx.x; i < v.plane_elems; i += blockDim.x) plane[i] = mk<C>(0, 0);
+  const int rs = v.row_start[k * (v.nslots + 1) + slot];
+  const int nrows = v.row_start[k * (v.nslots + 1) + slot + 1] - rs;
+  for (int i = threadIdx.x; i < nrows; i += blockDim.x) rows[i] = v.rows[rs + i];
+  __syncthreads();
+  const int es = v.entry_start[k * (v.nslots + 1) + slot];
+  const int ee = v.entry_start[k * (v.nslots + 1) + slot + 1];
+  for (int t = es + threadIdx.x; t < ee; t += blockDim.x) {
+    const int2 en = v.entries[t];
+    plane[en.y] = src[en.x];
+  }
+  __syncthreads();
+  dft_rows<+1>(plane, v.n3, v.A3, v.B3, v.n3, rows, nrows, stz);
+  dft_cols<+1>(plane, v.n2, v.A2, v.B2, v.n3, sty);
+  C* dst = work + (int64_t)gb * v.band_elems + (int64_t)slot * v.plane_elems;
+  for (int64_t i = threadIdx.x; i < v.plane_elems; i += blockDim.x) dst[i] = plane[i];
+}
+
+template <typename T>
+__global__ void stage_b_kernel(HpsiView v, const cx_t<T>* __restrict__ tw_xb,
+                               const cx_t<T>* __restrict__ tw_xf, const T* __restrict__ vpot,
+                               cx_t<T>* __restrict__ work) {
+  using C = cx_t<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* slab = reinterpret_cast<C*>(smem_raw);  // [n1][n3]
+  C* twb = slab + (int64_t)v.n1 * v.n3;
+  C* twf = twb + v.n1;
+  const int y = blockIdx.x;
+  const int gb = blockIdx.y;
+  load_twiddles(twb, tw_xb, v.n1);
+  load_twiddles(twf, tw_xf, v.n1);
+  C* wb = work + (int64_t)gb * v.band_elems + (int64_t)y * v.n3;
+  const int total = v.n1 * v.n3;
+  for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    const int x = e / v.n3, z = e % v.n3;
+    const int slot = v.slot_of_x[x];
+    slab[e] = slot >= 0 ? wb[(int64_t)slot * v.plane_elems + z] : mk<C>(0, 0);
+  }
+  __syncthreads();
+  dft_cols<+1>(slab, v.n1, v.A1, v.B1, v.n3, twb);
+  const T* vy = vpot + (int64_t)y * v.n3;
+  const int64_t xstride = (int64_t)v.n2 * v.n3;
+  for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    const int x = e / v.n3, z = e % v.n3;
+    slab[e] = cscale(slab[e], vy[x * xstride + z]);
+  }
+  __syncthreads();
+  dft_cols<-1>(slab, v.n1, v.A1, v.B1, v.n3, twf);
+  const int ts = v.nslots * v.n3;
+  for (int e = threadIdx.x; e < ts; e += blockDim.x) {
+    const int slot = e / v.n3, z = e % v.n3;
+    wb[(int64_t)slot * v.plane_elems + z] = slab[v.plane_x[slot] * v.n3 + z];
+  }
+}
+
+template <typename T>
+__global__ void stage_c_kernel(HpsiView v, const cx_t<T>* __restrict__ tw_y,
+                               const cx_t<T>* __restrict__ tw_z, const T* __restrict__ kin,
+                               const cx_t<T>* __restrict__ psi, const cx_t<T>* __restrict__ work,
+                               cx_t<T>* __restrict__ hpsi) {
+  using C = cx_t<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* plane = reinterpret_cast<C*>(smem_raw);
+  C* sty = plane + v.plane_elems;
+  C* stz = sty + v.n2;
+  int* rows = reinterpret_cast<int*>(stz + v.n3);
+
+  const int slot = blockIdx.x;
+  const int gb = blockIdx.y;
+  const int kl = gb / v.nbands, band = gb % v.nbands;
+  const int k = v.k_first + kl;
+  const int npw = v.npw[k];
+  const int64_t boff = (v.pw_off[k] - v.pw_off[v.k_first]) * v.nbands + (int64_t)band * npw;
+
+  load_twiddles(sty, tw_y, v.n2);
+  load_twiddles(stz, tw_z, v.n3);
+  const C* srcw = work + (int64_t)gb * v.band_elems + (int64_t)slot * v.plane_elems;
+  for (int64_t i = threadIdx.x; i < v.plane_elems; i += blockDim.x) plane[i] = srcw[i];
+  const int rs = v.row_start[k * (v.nslots + 1) + slot];
+  const int nrows = v.row_start[k * (v.nslots + 1) + slot + 1] - rs;
+  for (int i = threadIdx.x; i < nrows; i += blockDim.x) rows[i] = v.rows[rs + i];
+  __syncthreads();
+  dft_cols<-1>(plane, v.n2, v.A2, v.B2, v.n3, sty);
+  dft_rows<-1>(plane, v.n3, v.A3, v.B3, v.n3, rows, nrows, stz);
+  const int es = v.entry_start[k * (v.nslots + 1) + slot];
+  const int ee = v.entry_start[k * (v.nslots + 1) + slot + 1];
+  const T* kk = kin + v.pw_off[k];
+  for (int t = es + threadIdx.x; t < ee; t += blockDim.x) {
+    const int2 en = v.entries[t];
+    const C p = psi[boff + en.x];
+    C r = plane[en.y];
+    const T tg = kk[en.x];
+    r.x += tg * p.x;
+    r.y += tg * p.y;
+    hpsi[boff + en.x] = r;
+  }
+}
+
+// density: backward transform as stage A, x backward as in stage B, then |u|^2 weighted
+// accumulation into a permuted FP64 grid (one CTA per (y, band) slab, atomics per point).
+template <typename T>
+__global__ void density_b_kernel(HpsiView v, const cx_t<T>* __restrict__ tw_xb,
+                                 const cx_t<T>* __restrict__ work, const double* __restrict__ w,
+                                 double* __restrict__ acc) {
+  using C = cx_t<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* slab = reinterpret_cast<C*>(smem_raw);
+  C* twb = slab + (int64_t)v.n1 * v.n3;
+  const int y = blockIdx.x;
+  const int gb = blockIdx.y;
+  const double weight = w[gb];
+  if (weight == 0.0) return;
+  load_twiddles(twb, tw_xb, v.n1);
+  const C* wb = work + (int64_t)gb * v.band_elems + (int64_t)y * v.n3;
+  const int total = v.n1 * v.n3;
+  for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    const int x = e / v.n3, z = e % v.n3;
+    const int slot = v.slot_of_x[x];
+    slab[e] = slot >= 0 ? wb[(int64_t)slot * v.plane_elems + z] : mk<C>(0, 0);
+  }
+  __syncthreads();
+  dft_cols<+1>(slab, v.n1, v.A1, v.B1, v.n3, twb);
+  const int64_t xstride = (int64_t)v.n2 * v.n3;
+  for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    const int x = e / v.n3, z = e % v.n3;
+    const C u = slab[e];
+    const double m2 = (double)u.x * (double)u.x + (double)u.y * (double)u.y;
+    atomicAdd(acc + x * xstride + (int64_t)y * v.n3 + z, weight * m2);
+  }
+}
+
+template <typename T>
+__global__ void permute_potential_kernel(const double* __restrict__ v, T* __restrict__ out,
+                                         int n1, int n2, int n3, int A1, int B1, int A2, int B2,
+                                         int A3, int B3, double scale) {
+  const int64_t N = (int64_t)n1 * n2 * n3;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < N;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int p3 = e % n3, p2 = (e / n3) % n2, p1 = e / ((int64_t)n2 * n3);
+    const int x = p1 / B1 + A1 * (p1 % B1);
+    const int y = p2 / B2 + A2 * (p2 % B2);
+    const int z = p3 / B3 + A3 * (p3 % B3);
+    out[e] = (T)(v[((int64_t)x * n2 + y) * n3 + z] * scale);
+  }
+}
+
+__global__ void unpermute_add_kernel(const double* __restrict__ acc, double* __restrict__ rho,
+                                     int n1, int n2, int n3, int A1, int B1, int A2, int B2,
+                                     int A3, int B3) {
+  const int64_t N = (int64_t)n1 * n2 * n3;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < N;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int p3 = e % n3, p2 = (e / n3) % n2, p1 = e / ((int64_t)n2 * n3);
+    const int x = p1 / B1 + A1 * (p1 % B1);
+    const int y = p2 / B2 + A2 * (p2 % B2);
+    const int z = p3 / B3 + A3 * (p3 % B3);
+    rho[((int64_t)x * n2 + y) * n3 + z] += acc[e];
+  }
+}
+
+// Batch functors for the nonlocal products over k-points of one call.
+template <typename C> struct ProjectBatch {  // P_k = psi_k B_k^H  (nbands x nproj)
+  const C* psi; const C* proj; C* out; const int64_t* pw_off; const int* npw;
+  int k_first, nbands, nproj;
+  __device__ GemmProblem<C> operator()(int z) const {
+    const int k = k_first + z;
+    const int64_t off = pw_off[k] - pw_off[k_first];
+    GemmProblem<C> p;
+    p.a = psi + off * nbands; p.b = proj + pw_off[k] * nproj; p.c = out + (int64_t)z * nbands * nproj;
+    p.m = nbands; p.n = nproj; p.k = npw[k];
+    p.lda = npw[k]; p.ldb = npw[k]; p.ldc = nproj;
+    return p;
+  }
+};
+template <typename C> struct ApplyBatch {    // hpsi_k += P_k (D B_k)  (nbands x npw_k)
+  const C* pmat; const C* dproj; C* out; const int64_t* pw_off; const int* npw;
+  int k_first, nbands, nproj;
+  __device__ GemmProblem<C> operator()(int z) const {
+    const int k = k_first + z;
+    const int64_t off = pw_off[k] - pw_off[k_first];
+    GemmProblem<C> p;
+    p.a = pmat + (int64_t)z * nbands * nproj; p.b = dproj + pw_off[k] * nproj; p.c = out + off * nbands;
+    p.m = nbands; p.n = npw[k]; p.k = nproj;
+    p.lda = nproj; p.ldb = npw[k]; p.ldc = npw[k];
+    return p;
+  }
+};
+
+HpsiView make_view(const AmaEngine* e, int k_first, int nbands) {
+  HpsiView v;
+  v.n1 = e->ax[0].n; v.n2 = e->ax[1].n; v.n3 = e->ax[2].n;
+  v.A1 = e->ax[0].A; v.B1 = e->ax[0].B; v.A2 = e->ax[1].A; v.B2 = e->ax[1].B;
+  v.A3 = e->ax[2].A; v.B3 = e->ax[2].B;
+  v.nslots = e->nslots;
+  v.plane_x = e->d.plane_x; v.slot_of_x = e->d.slot_of_x; v.entries = e->d.entries;
+  v.entry_start = e->d.entry_start; v.rows = e->d.rows; v.row_start = e->d.row_start;
+  v.pw_off = e->d.pw_off; v.npw = e->d.npw;
+  v.k_first = k_first; v.nbands = nbands;
+  v.plane_elems = (int64_t)v.n2 * v.n3;
+  v.band_elems = v.plane_elems * v.nslots;
+  return v;
+}
+
+constexpr int kStageThreads = 256;
+
+template <typename T>
+size_t plane_smem(const AmaEngine* e) {
+  return (size_t)(e->ax[1].n * e->ax[2].n + e->ax[1].n + e->ax[2].n) * sizeof(cx_t<T>) +
+         (size_t)e->ax[1].n * sizeof(int);
+}
+template <typename T>
+size_t slab_smem(const AmaEngine* e) {
+  return (size_t)(e->ax[0].n * e->ax[2].n + 2 * e->ax[0].n) * sizeof(cx_t<T>);
+}
+
+template <typename T>
+int set_smem_limits(const AmaEngine* e) {
+  const size_t ps = plane_smem<T>(e), ss = slab_smem<T>(e);
+  int dev = 0, optin = 0;
+  AMA_CUDA_TRY(cudaGetDevice(&dev));
+  AMA_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  AMA_REQUIRE(ps <= (size_t)optin && ss <= (size_t)optin, AMA_ERR_UNSUPPORTED,
+              "grid plane does not fit in shared memory at this precision");
+  AMA_CUDA_TRY(cudaFuncSetAttribute(stage_a_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
+  AMA_CUDA_TRY(cudaFuncSetAttribute(stage_c_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
+  AMA_CUDA_TRY(cudaFuncSetAttribute(stage_b_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
+  AMA_CUDA_TRY(cudaFuncSetAttribute(density_b_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
+  return AMA_OK;
+}
+
+int prec_ok(const AmaEngine* e, int precision) {
+  AMA_REQUIRE(precision == AMA_C64 || precision == AMA_C128, AMA_ERR_ARG, "precision must be AMA_C64 or AMA_C128");
+  AMA_REQUIRE(e->precisions & (1u << precision), AMA_ERR_ARG,
+              "the engine was created without this precision");
+  return AMA_OK;
+}
+
+int ensure_work(AmaEngine* e, int precision, int64_t bands) {
+  const size_t el = precision == AMA_C64 ? sizeof(float2) : sizeof(double2);
+  const size_t need = (size_t)bands * e->nslots * e->ax[1].n * e->ax[2].n * el;
+  AMA_CUDA_TRY(grow<char>(&e->work[precision], &e->work_bytes[precision], need));
+  return AMA_OK;
+}
+
+template <typename T>
+int run_fft_stages_a(AmaEngine* e, const HpsiView& v, int nb_total, const void* psi, cudaStream_t s) {
+  using C = cx_t<T>;
+  const int p = std::is_same<T, float>::value ? AMA_C64 : AMA_C128;
+  dim3 ga(e->nslots, nb_total);
+  stage_a_kernel<T><<<ga, kStageThreads, plane_smem<T>(e), s>>>(
+      v, (const C*)e->d.tw[p][1][0], (const C*)e->d.tw[p][2][0], (const C*)psi, (C*)e->work[p]);
+  AMA_CHECK_LAUNCH();
+  return AMA_OK;
+}
+
+template <typename T>
+int hpsi_impl(AmaEngine* e, int k_first, int k_count, int nbands, int spin, const void* psi,
+              void* hpsi, cudaStream_t s) {
+  using C = cx_t<T>;
+  const int p = std::is_same<T, float>::value ? AMA_C64 : AMA_C128;
+  const int64_t nb_total = (int64_t)k_count * nbands;
+  AMA_REQUIRE(nb_total <= 65535, AMA_ERR_UNSUPPORTED, "more than 65535 bands in one H.psi call");
+  int rc = ensure_work(e, p, nb_total);
+  if (rc) return rc;
+  HpsiView v = make_view(e, k_first, nbands);
+  const T* vpot = (p == AMA_C64 ? (const T*)e->d.v32 : (const T*)e->d.v64) + (int64_t)spin * e->N;
+  const T* kin = p == AMA_C64 ? (const T*)e->d.kin32 : (const T*)e->d.kin64;
+
+  rc = run_fft_stages_a<T>(e, v, (int)nb_total, psi, s);
+  if (rc) return rc;
+  dim3 gb(e->ax[1].n, nb_total);
+  stage_b_kernel<T><<<gb, kStageThreads, slab_smem<T>(e), s>>>(
+      v, (const C*)e->d.tw[p][0][0], (const C*)e->d.tw[p][0][1], vpot, (C*)e->work[p]);
+  AMA_CHECK_LAUNCH();
+  dim3 gc(e->nslots, nb_total);
+  stage_c_kernel<T><<<gc, kStageThreads, plane_smem<T>(e), s>>>(
+      v, (const C*)e->d.tw[p][1][1], (const C*)e->d.tw[p][2][1], kin, (const C*)psi,
+      (const C*)e->work[p], (C*)hpsi);
+  AMA_CHECK_LAUNCH();
+
+  if (e->nproj > 0) {
+    const size_t el = sizeof(C);
+    const size_t pbytes = (size_t)nb_total * e->nproj * el;
+    AMA_CUDA_TRY(grow<char>(&e->ws_proj[p], &e->ws_proj_bytes[p], pbytes));
+    int maxnpw = 0;
+    for (int k = k_first; k < k_first + k_count; ++k) maxnpw = std::max(maxnpw, e->npw[k]);
+    // split the long npw reduction so that the tile grid covers the GPU several times
+    const int tiles = ((nbands + kBM - 1) / kBM) * ((e->nproj + kBN - 1) / kBN) * k_count;
+    int splits = std::max(1, std::min(64, (4 * 148 + tiles - 1) / tiles));
+    splits = std::min(splits, std::max(1, maxnpw / 256));
+    const int64_t pstride = (int64_t)nbands * e->nproj;
+    if (splits > 1)
+      AMA_CUDA_TRY(grow<char>(&e->ws_part[p], &e->ws_part_bytes[p], (size_t)k_count * splits * pstride * el));
+    ProjectBatch<C> pb{(const C*)psi, (const C*)e->d.proj[p], (C*)e->ws_proj[p], e->d.pw_off, e->d.npw,
+                       k_first, nbands, e->nproj};
+    AMA_CUDA_TRY((launch_cgemm<T, kNC>(pb, k_count, nbands, e->nproj, splits, mk<C>(1, 0), mk<C>(0, 0),
+                                       (C*)e->ws_part[p], pstride, s)));
+    ApplyBatch<C> ab{(const C*)e->ws_proj[p], (const C*)e->d.dproj[p], (C*)hpsi, e->d.pw_off, e->d.npw,
+                     k_first, nbands, e->nproj};
+    AMA_CUDA_TRY((launch_cgemm<T, kNN>(ab, k_count, nbands, maxnpw, 1, mk<C>(1, 0), mk<C>(1, 0),
+                                       nullptr, 0, s)));
+  }
+  return AMA_OK;
+}
+
+template <typename T>
+int density_impl(AmaEngine* e, int k_first, int k_count, int nbands, const void* psi,
+                 const double* weights, double* rho, cudaStream_t s) {
+  using C = cx_t<T>;
+  const int p = std::is_same<T, float>::value ? AMA_C64 : AMA_C128;
+  const int64_t nb_total = (int64_t)k_count * nbands;
+  AMA_REQUIRE(nb_total <= 65535, AMA_ERR_UNSUPPORTED, "more than 65535 bands in one density call");
+  int rc = ensure_work(e, p, nb_total);
+  if (rc) return rc;
+  AMA_CUDA_TRY(grow<char>((void**)&e->ws_dens, &e->ws_dens_bytes, (size_t)e->N * sizeof(double)));
+  AMA_CUDA_TRY(cudaMemsetAsync(e->ws_dens, 0, (size_t)e->N * sizeof(double), s));
+  HpsiView v = make_view(e, k_first, nbands);
+  rc = run_fft_stages_a<T>(e, v, (int)nb_total, psi, s);
+  if (rc) return rc;
+  dim3 gb(e->ax[1].n, nb_total);
+  density_b_kernel<T><<<gb, kStageThreads, slab_smem<T>(e), s>>>(v, (const C*)e->d.tw[p][0][0],
+                                                                  (const C*)e->work[p], weights, e->ws_dens);
+  AMA_CHECK_LAUNCH();
+  unpermute_add_kernel<<<592, 256, 0, s>>>(e->ws_dens, rho, e->ax[0].n, e->ax[1].n, e->ax[2].n,
+                                           e->ax[0].A, e->ax[0].B, e->ax[1].A, e->ax[1].B, e->ax[2].A,
+                                           e->ax[2].B);
+  AMA_CHECK_LAUNCH();
+  return AMA_OK;
+}
+
+template <typename T>
+int upload_twiddles(AmaEngine* e, int prec) {
+  using C = cx_t<T>;
+  for (int a = 0; a < 3; ++a) {
+    const int n = e->ax[a].n;
+    for (int dir = 0; dir < 2; ++dir) {
+      const double sign = dir == 0 ? 1.0 : -1.0;
+      std::vector<C> h(n);
+      for (int t = 0; t < n; ++t) {
+        const double ang = 2.0 * M_PI * (double)t / (double)n;
+        h[t] = mk<C>(std::cos(ang), sign * std::sin(ang));
+      }
+      C* dptr = nullptr;
+      int rc = upload(&dptr, h.data(), h.size());
+      if (rc) return rc;
+      e->d.tw[prec][a][dir] = dptr;
+    }
+  }
+  return AMA_OK;
+}
+
+void free_grid_filters(const AmaEngine* e);
+
+void free_engine(AmaEngine* e) {
+  free_grid_filters(e);
+  auto f = [](void* p) { if (p) cudaFree(p); };
+  f(e->d.plane_x); f(e->d.slot_of_x); f(e->d.entries); f(e->d.entry_start); f(e->d.rows);
+  f(e->d.row_start); f(e->d.pw_off); f(e->d.npw); f(e->d.kin64); f(e->d.kin32); f(e->d.v64); f(e->d.v32);
+  for (int p = 0; p < 2; ++p) {
+    for (int a = 0; a < 3; ++a) for (int d = 0; d < 2; ++d) f(e->d.tw[p][a][d]);
+    f(e->d.proj[p]); f(e->d.dproj[p]); f(e->work[p]); f(e->ws_proj[p]); f(e->ws_part[p]);
+  }
+  f(e->ws_dens);
+  delete e;
+}
+
+}  // namespace
+
+// ===================================================================== C-ABI
+extern "C" int ama_engine_create(const AmaSystemDesc* desc, AmaEngine** out) {
+  AMA_REQUIRE(desc && out, AMA_ERR_ARG, "null argument");
+  *out = nullptr;
+  AMA_REQUIRE(desc->nk >= 1 && desc->npw && desc->miller && desc->kinetic, AMA_ERR_ARG,
+              "desc needs nk >= 1, npw, miller and kinetic");
+  AMA_REQUIRE(desc->nspin == 1 || desc->nspin == 2, AMA_ERR_ARG, "nspin must be 1 or 2");
+  AMA_REQUIRE(desc->nproj >= 0 && (desc->nproj == 0 || (desc->projectors && desc->dij)), AMA_ERR_ARG,
+              "projectors and dij are required when nproj > 0");
+  AMA_REQUIRE((desc->precisions & 3u) != 0, AMA_ERR_ARG, "no precision requested");
+  AmaEngine* e = new AmaEngine();
+  const int dims[3] = {desc->n1, desc->n2, desc->n3};
+  for (int a = 0; a < 3; ++a) {
+    if (dims[a] < 1 || !split_length(dims[a], &e->ax[a])) {
+      delete e;
+      ama::set_error("grid length " + std::to_string(dims[a]) +
+                     " is not a product of two codelet lengths (1..16, no 13)");
+      return AMA_ERR_UNSUPPORTED;
+    }
+  }
+  const int n1 = dims[0], n2 = dims[1], n3 = dims[2];
+  e->N = (int64_t)n1 * n2 * n3;
+  e->nk = desc->nk;
+  e->nspin = desc->nspin;
+  e->nproj = desc->nproj;
+  e->precisions = desc->precisions & 3u;
+  e->npw.assign(desc->npw, desc->npw + desc->nk);
+  e->pw_off.assign(e->nk + 1, 0);
+  for (int k = 0; k < e->nk; ++k) {
+    if (e->npw[k] < 1) { delete e; ama::set_error("npw must be positive"); return AMA_ERR_SHAPE; }
+    e->pw_off[k + 1] = e->pw_off[k] + e->npw[k];
+    e->max_npw = std::max(e->max_npw, e->npw[k]);
+  }
+  const int64_t total_pw = e->pw_off[e->nk];
+
+  // x-plane slots: every natural x index that any k-point's sphere touches
+  std::vector<int> x_used(n1, 0);
+  for (int64_t g = 0; g < total_pw; ++g) {
+    const int h = desc->miller[3 * g], kk = desc->miller[3 * g + 1], l = desc->miller[3 * g + 2];
+    if (2 * std::abs(h) + 1 > n1 || 2 * std::abs(kk) + 1 > n2 || 2 * std::abs(l) + 1 > n3) {
+      delete e;
+      ama::set_error("grid is too small for the Miller indices of the spheres");
+      return AMA_ERR_SHAPE;
+    }
+    x_used[((h % n1) + n1) % n1] = 1;
+  }
+  std::vector<int> plane_x, slot_of_x(n1, -1);
+  for (int x = 0; x < n1; ++x)
+    if (x_used[x]) { slot_of_x[x] = (int)plane_x.size(); plane_x.push_back(x); }
+  e->nslots = (int)plane_x.size();
+  const int ns = e->nslots;
+
+  // per (k, slot): sphere entries and the y rows they occupy
+  std::vector<int2> entries(total_pw);
+  std::vector<int> entry_start((size_t)e->nk * (ns + 1));
+  std::vector<int> rows, row_start((size_t)e->nk * (ns + 1));
+  for (int k = 0; k < e->nk; ++k) {
+    const int64_t base = e->pw_off[k];
+    const int np = e->npw[k];
+    std::vector<int> count(ns, 0);
+    std::vector<int> slot_g(np), pos_g(np);
+    for (int g = 0; g < np; ++g) {
+      const int32_t* m = desc->miller + 3 * (base + g);
+      const int x = ((m[0] % n1) + n1) % n1, y = ((m[1] % n2) + n2) % n2, z = ((m[2] % n3) + n3) % n3;
+      slot_g[g] = slot_of_x[x];
+      pos_g[g] = y * n3 + z;
+      count[slot_g[g]]++;
+    }
+    std::vector<int> start(ns + 1, 0);
+    for (int s = 0; s < ns; ++s) start[s + 1] = start[s] + count[s];
+    std::vector<int> fill(start.begin(), start.end() - 1);
+    for (int g = 0; g < np; ++g) {
+      const int s = slot_g[g];
+      entries[base + fill[s]++] = make_int2(g, pos_g[g]);
+    }
+    for (int s = 0; s <= ns; ++s) entry_start[(size_t)k * (ns + 1) + s] = (int)(base + start[s]);
+    for (int s = 0; s < ns; ++s) {
+      row_start[(size_t)k * (ns + 1) + s] = (int)rows.size();
+      std::vector<char> used(n2, 0);
+      for (int t = start[s]; t < start[s + 1]; ++t) used[entries[base + t].y / n3] = 1;
+      int cnt = 0;
+      for (int y = 0; y < n2; ++y) if (used[y]) { rows.push_back(y); ++cnt; }
+      e->max_rows = std::max(e->max_rows, cnt);
+    }
+    row_start[(size_t)k * (ns + 1) + ns] = (int)rows.size();
+  }
+
+  int rc = AMA_OK;
+  std::vector<float> kin32(desc->kinetic, desc->kinetic + total_pw);
+  std::vector<int64_t> pw_off(e->pw_off);
+  if ((rc = upload(&e->d.plane_x, plane_x.data(), plane_x.size())) ||
+      (rc = upload(&e->d.slot_of_x, slot_of_x.data(), slot_of_x.size())) ||
+      (rc = upload(&e->d.entries, entries.data(), entries.size())) ||
+      (rc = upload(&e->d.entry_start, entry_start.data(), entry_start.size())) ||
+      (rc = upload(&e->d.rows, rows.data(), rows.size())) ||
+      (rc = upload(&e->d.row_start, row_start.data(), row_start.size())) ||
+      (rc = upload(&e->d.pw_off, pw_off.data(), pw_off.size())) ||
+      (rc = upload(&e->d.npw, e->npw.data(), e->npw.size())) ||
+      (rc = upload(&e->d.kin64, desc->kinetic, (size_t)total_pw)) ||
+      (rc = upload(&e->d.kin32, kin32.data(), kin32.size()))) {
+    free_engine(e);
+    return rc;
+  }
+  for (int p = 0; p < 2; ++p) {
+    if (!(e->precisions & (1u << p))) continue;
+    rc = p == AMA_C64 ? upload_twiddles<float>(e, p) : upload_twiddles<double>(e, p);
+    if (!rc) rc = p == AMA_C64 ? set_smem_limits<float>(e) : set_smem_limits<double>(e);
+    if (rc) { free_engine(e); return rc; }
+  }
+  if (e->nproj > 0) {
+    // D.B per k on the host: D is block-diagonal, so loop over its nonzeros only.
+    const int np = e->nproj;
+    std::vector<std::vector<std::pair<int, double>>> dnz(np);
+    for (int i = 0; i < np; ++i)
+      for (int j = 0; j < np; ++j)
+        if (desc->dij[(size_t)i * np + j] != 0.0) dnz[i].push_back({j, desc->dij[(size_t)i * np + j]});
+    const size_t nel = (size_t)total_pw * np;
+    std::vector<double> db(2 * nel, 0.0);
+    for (int k = 0; k < e->nk; ++k) {
+      const size_t kb = (size_t)e->pw_off[k] * np;
+      const int npk = e->npw[k];
+      for (int i = 0; i < np; ++i) {
+        double* dst = db.data() + 2 * (kb + (size_t)i * npk);
+        for (auto& jd : dnz[i]) {
+          const double* src = desc->projectors + 2 * (kb + (size_t)jd.first * npk);
+          for (int g = 0; g < 2 * npk; ++g) dst[g] += jd.second * src[g];
+        }
+      }
+    }
+    for (int p = 0; p < 2 && !rc; ++p) {
+      if (!(e->precisions & (1u << p))) continue;
+      if (p == AMA_C128) {
+        double2* b = nullptr; double2* d = nullptr;
+        rc = upload(&b, (const double2*)desc->projectors, nel);
+        if (!rc) rc = upload(&d, (const double2*)db.data(), nel);
+        e->d.proj[p] = b; e->d.dproj[p] = d;
+      } else {
+        std::vector<float2> bf(nel), df(nel);
+        for (size_t i = 0; i < nel; ++i) {
+          bf[i] = make_float2((float)desc->projectors[2 * i], (float)desc->projectors[2 * i + 1]);
+          df[i] = make_float2((float)db[2 * i], (float)db[2 * i + 1]);
+        }
+        float2* b = nullptr; float2* d = nullptr;
+        rc = upload(&b, bf.data(), nel);
+        if (!rc) rc = upload(&d, df.data(), nel);
+        e->d.proj[p] = b; e->d.dproj[p] = d;
+      }
+    }
+    if (rc) { free_engine(e); return rc; }
+  }
+  *out = e;
+  return AMA_OK;
+}
+
+extern "C" int ama_engine_destroy(AmaEngine* e) {
+  if (!e) return AMA_OK;
+  cudaDeviceSynchronize();
+  free_engine(e);
+  return AMA_OK;
+}
+
+extern "C" int ama_set_potential(AmaEngine* e, const double* v, int32_t nspin, void* stream) {
+  AMA_REQUIRE(e && v, AMA_ERR_ARG, "null argument");
+  AMA_REQUIRE(nspin == e->nspin, AMA_ERR_SHAPE, "potential spin channels do not match the engine");
+  cudaStream_t s = (cudaStream_t)stream;
+  const int64_t N = e->N;
+  if (!e->d.v64 && (e->precisions & (1u << AMA_C128)))
+    AMA_CUDA_TRY(cudaMalloc((void**)&e->d.v64, (size_t)nspin * N * sizeof(double)));
+  if (!e->d.v32 && (e->precisions & (1u << AMA_C64)))
+    AMA_CUDA_TRY(cudaMalloc((void**)&e->d.v32, (size_t)nspin * N * sizeof(float)));
+  const double scale = 1.0 / (double)N;
+  for (int sp = 0; sp < nspin; ++sp) {
+    if (e->d.v64)
+      permute_potential_kernel<double><<<592, 256, 0, s>>>(v + sp * N, e->d.v64 + sp * N, e->ax[0].n, e->ax[1].n,
+                                                           e->ax[2].n, e->ax[0].A, e->ax[0].B, e->ax[1].A,
+                                                           e->ax[1].B, e->ax[2].A, e->ax[2].B, scale);
+    if (e->d.v32)
+      permute_potential_kernel<float><<<592, 256, 0, s>>>(v + sp * N, e->d.v32 + sp * N, e->ax[0].n, e->ax[1].n,
+                                                          e->ax[2].n, e->ax[0].A, e->ax[0].B, e->ax[1].A,
+                                                          e->ax[1].B, e->ax[2].A, e->ax[2].B, scale);
+  }
+  AMA_CHECK_LAUNCH();
+  e->has_potential = true;
+  return AMA_OK;
+}
+
+extern "C" int ama_reserve(AmaEngine* e, int32_t precision, int64_t max_bands) {
+  AMA_REQUIRE(e, AMA_ERR_ARG, "null engine");
+  int rc = prec_ok(e, precision);
+  if (rc) return rc;
+  return ensure_work(e, precision, max_bands);
+}
+
+static int check_call(AmaEngine* e, int precision, int k_first, int k_count, int nbands) {
+  AMA_REQUIRE(e, AMA_ERR_ARG, "null engine");
+  int rc = prec_ok(e, precision);
+  if (rc) return rc;
+  AMA_REQUIRE(k_first >= 0 && k_count >= 1 && k_first + k_count <= e->nk, AMA_ERR_SHAPE,
+              "k-point range outside the engine's k-points");
+  AMA_REQUIRE(nbands >= 1, AMA_ERR_SHAPE, "nbands must be positive");
+  return AMA_OK;
+}
+
+extern "C" int ama_hpsi(AmaEngine* e, int32_t precision, int32_t k_first, int32_t k_count,
+                        int32_t nbands, int32_t spin, const void* psi, void* hpsi, void* stream) {
+  int rc = check_call(e, precision, k_first, k_count, nbands);
+  if (rc) return rc;
+  AMA_REQUIRE(psi && hpsi, AMA_ERR_ARG, "null psi/hpsi");
+  AMA_REQUIRE(psi != hpsi, AMA_ERR_ARG, "hpsi must not alias psi");
+  AMA_REQUIRE(spin >= 0 && spin < e->nspin, AMA_ERR_ARG, "spin out of range");
+  AMA_REQUIRE(e->has_potential, AMA_ERR_ARG, "ama_set_potential has not been called");
+  cudaStream_t s = (cudaStream_t)stream;
+  return precision == AMA_C64 ? hpsi_impl<float>(e, k_first, k_count, nbands, spin, psi, hpsi, s)
+                              : hpsi_impl<double>(e, k_first, k_count, nbands, spin, psi, hpsi, s);
+}
+
+extern "C" int ama_density_accumulate(AmaEngine* e, int32_t precision, int32_t k_first,
+                                      int32_t k_count, int32_t nbands, const void* psi,
+                                      const double* weights, double* rho, void* stream) {
+  int rc = check_call(e, precision, k_first, k_count, nbands);
+  if (rc) return rc;
+  AMA_REQUIRE(psi && weights && rho, AMA_ERR_ARG, "null argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  return precision == AMA_C64 ? density_impl<float>(e, k_first, k_count, nbands, psi, weights, rho, s)
+                              : density_impl<double>(e, k_first, k_count, nbands, psi, weights, rho, s);
+}
+
+template <typename T>
+static int project_impl(AmaEngine* e, int k, int nbands, const void* psi, void* out, cudaStream_t s) {
+  using C = cx_t<T>;
+  const int p = std::is_same<T, float>::value ? AMA_C64 : AMA_C128;
+  const int tiles = ((nbands + kBM - 1) / kBM) * ((e->nproj + kBN - 1) / kBN);
+  int splits = std::max(1, std::min(64, (4 * 148 + tiles - 1) / tiles));
+  splits = std::min(splits, std::max(1, e->npw[k] / 256));
+  const int64_t pstride = (int64_t)nbands * e->nproj;
+  if (splits > 1)
+    AMA_CUDA_TRY(grow<char>(&e->ws_part[p], &e->ws_part_bytes[p], (size_t)splits * pstride * sizeof(C)));
+  ProjectBatch<C> pb{(const C*)psi, (const C*)e->d.proj[p], (C*)out, e->d.pw_off, e->d.npw, k, nbands, e->nproj};
+  AMA_CUDA_TRY((launch_cgemm<T, kNC>(pb, 1, nbands, e->nproj, splits, mk<C>(1, 0), mk<C>(0, 0),
+                                     (C*)e->ws_part[p], pstride, s)));
+  return AMA_OK;
+}
+
+extern "C" int ama_project(AmaEngine* e, int32_t precision, int32_t k, int32_t nbands,
+                           const void* psi, void* proj, void* stream) {
+  int rc = check_call(e, precision, k, 1, nbands);
+  if (rc) return rc;
+  AMA_REQUIRE(psi && proj, AMA_ERR_ARG, "null argument");
+  AMA_REQUIRE(e->nproj > 0, AMA_ERR_SHAPE, "the engine has no projectors");
+  cudaStream_t s = (cudaStream_t)stream;
+  return precision == AMA_C64 ? project_impl<float>(e, k, nbands, psi, proj, s)
+                              : project_impl<double>(e, k, nbands, psi, proj, s);
+}
+
+// ============================================================ grid filters
+// out(r) = Re sum_G f(G) rho(G) e^{iGr},  rho(G) = (1/N) sum_r rho(r) e^{-iGr},
+// energy += sum_G f_e(G) |rho(G)|^2. Three stages like H.psi but over every plane:
+// G1 forward z,y per x-plane; G2 forward x, filter, backward x per y; G3 backward y,z.
+// The filter is stored in the storage order of the forward transform's output.
+namespace {
+
+struct GridView {
+  int n1, n2, n3, A1, B1, A2, B2, A3, B3;
+  int64_t plane_elems;
+};
+
+GridView grid_view(const AmaEngine* e) {
+  GridView g;
+  g.n1 = e->ax[0].n; g.n2 = e->ax[1].n; g.n3 = e->ax[2].n;
+  g.A1 = e->ax[0].A; g.B1 = e->ax[0].B; g.A2 = e->ax[1].A; g.B2 = e->ax[1].B;
+  g.A3 = e->ax[2].A; g.B3 = e->ax[2].B;
+  g.plane_elems = (int64_t)g.n2 * g.n3;
+  return g;
+}
+
+__global__ void grid_g1_kernel(GridView g, const double2* tw_y, const double2* tw_z,
+                               const double* __restrict__ in, double2* __restrict__ work) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* plane = reinterpret_cast<double2*>(smem_raw);
+  double2* sty = plane + g.plane_elems;
+  double2* stz = sty + g.n2;
+  int* rows = reinterpret_cast<int*>(stz + g.n3);
+  const int x = blockIdx.x;
+  load_twiddles(sty, tw_y, g.n2);
+  load_twiddles(stz, tw_z, g.n3);
+  for (int i = threadIdx.x; i < g.n2; i += blockDim.x) rows[i] = i;
+  const double* src = in + (int64_t)x * g.plane_elems;
+  for (int64_t i = threadIdx.x; i < g.plane_elems; i += blockDim.x) plane[i] = make_double2(src[i], 0.0);
+  __syncthreads();
+  dft_rows<-1, true>(plane, g.n3, g.A3, g.B3, g.n3, rows, g.n2, stz);
+  dft_cols<-1, true>(plane, g.n2, g.A2, g.B2, g.n3, sty);
+  double2* dst = work + (int64_t)x * g.plane_elems;
+  for (int64_t i = threadIdx.x; i < g.plane_elems; i += blockDim.x) dst[i] = plane[i];
+}
+
+__global__ void grid_g2_kernel(GridView g, const double2* tw_f, const double2* tw_b,
+                               const double* __restrict__ filt, const double* __restrict__ efilt,
+                               double scale, double escale, double2* __restrict__ work,
+                               double* __restrict__ energy) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* slab = reinterpret_cast<double2*>(smem_raw);
+  double2* twf = slab + (int64_t)g.n1 * g.n3;
+  double2* twb = twf + g.n1;
+  __shared__ double red[32];
+  const int y = blockIdx.x;
+  load_twiddles(twf, tw_f, g.n1);
+  load_twiddles(twb, tw_b, g.n1);
+  double2* wb = work + (int64_t)y * g.n3;
+  const int total = g.n1 * g.n3;
+  for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    const int x = e / g.n3, z = e % g.n3;
+    slab[e] = wb[(int64_t)x * g.plane_elems + z];
+  }
+  __syncthreads();
+  dft_cols<-1, true>(slab, g.n1, g.A1, g.B1, g.n3, twf);
+  const int64_t xstride = g.plane_elems;
+  double acc = 0.0;
+  for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    const int x = e / g.n3, z = e % g.n3;
+    const int64_t gi = x * xstride + (int64_t)y * g.n3 + z;
+    const double2 c = slab[e];
+    if (efilt) acc += efilt[gi] * (c.x * c.x + c.y * c.y);
+    const double f = filt[gi] * scale;
+    slab[e] = make_double2(c.x * f, c.y * f);
+  }
+  if (energy) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  }
+  __syncthreads();
+  if (energy && threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    atomicAdd(energy, t * escale);
+  }
+  dft_cols<+1, false>(slab, g.n1, g.A1, g.B1, g.n3, twb);
+  for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    const int x = e / g.n3, z = e % g.n3;
+    wb[(int64_t)x * g.plane_elems + z] = slab[e];
+  }
+}
+
+__global__ void grid_g3_kernel(GridView g, const double2* tw_y, const double2* tw_z,
+                               const double2* __restrict__ work, double* __restrict__ out) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* plane = reinterpret_cast<double2*>(smem_raw);
+  double2* sty = plane + g.plane_elems;
+  double2* stz = sty + g.n2;
+  int* rows = reinterpret_cast<int*>(stz + g.n3);
+  const int x = blockIdx.x;
+  load_twiddles(sty, tw_y, g.n2);
+  load_twiddles(stz, tw_z, g.n3);
+  for (int i = threadIdx.x; i < g.n2; i += blockDim.x) rows[i] = i;
+  const double2* src = work + (int64_t)x * g.plane_elems;
+  for (int64_t i = threadIdx.x; i < g.plane_elems; i += blockDim.x) plane[i] = src[i];
+  __syncthreads();
+  dft_cols<+1, false>(plane, g.n2, g.A2, g.B2, g.n3, sty);
+  dft_rows<+1, false>(plane, g.n3, g.A3, g.B3, g.n3, rows, g.n2, stz);
+  double* dst = out + (int64_t)x * g.plane_elems;
+  for (int64_t i = threadIdx.x; i < g.plane_elems; i += blockDim.x) dst[i] = plane[i].x;
+}
+
+}  // namespace
+
+struct AmaGridFilters {
+  double* filt[4] = {};
+};
+static std::map<const AmaEngine*, AmaGridFilters> g_filters;
+namespace {
+void free_grid_filters(const AmaEngine* e) {
+  auto it = g_filters.find(e);
+  if (it == g_filters.end()) return;
+  for (double* p : it->second.filt) if (p) cudaFree(p);
+  g_filters.erase(it);
+}
+}  // namespace
+static double2* g_grid_work = nullptr;
+static size_t g_grid_work_bytes = 0;
+
+extern "C" int ama_set_grid_filter(AmaEngine* e, int32_t slot, const double* filter) {
+  AMA_REQUIRE(e && filter, AMA_ERR_ARG, "null argument");
+  AMA_REQUIRE(slot >= 0 && slot < 4, AMA_ERR_ARG, "filter slot must be 0..3");
+  AMA_REQUIRE(e->precisions & (1u << AMA_C128), AMA_ERR_ARG, "grid filters need the complex128 tables");
+  const int n1 = e->ax[0].n, n2 = e->ax[1].n, n3 = e->ax[2].n;
+  std::vector<double> perm((size_t)e->N);
+  for (int p1 = 0; p1 < n1; ++p1) {
+    const int x = p1 / e->ax[0].B + e->ax[0].A * (p1 % e->ax[0].B);
+    for (int p2 = 0; p2 < n2; ++p2) {
+      const int y = p2 / e->ax[1].B + e->ax[1].A * (p2 % e->ax[1].B);
+      for (int p3 = 0; p3 < n3; ++p3) {
+        const int z = p3 / e->ax[2].B + e->ax[2].A * (p3 % e->ax[2].B);
+        perm[((size_t)p1 * n2 + p2) * n3 + p3] = filter[((size_t)x * n2 + y) * n3 + z];
+      }
+    }
+  }
+  AmaGridFilters& f = g_filters[e];
+  if (!f.filt[slot]) AMA_CUDA_TRY(cudaMalloc((void**)&f.filt[slot], (size_t)e->N * sizeof(double)));
+  AMA_CUDA_TRY(cudaMemcpy(f.filt[slot], perm.data(), (size_t)e->N * sizeof(double), cudaMemcpyHostToDevice));
+  return AMA_OK;
+}
+
+extern "C" int ama_grid_filter(AmaEngine* e, int32_t slot, int32_t energy_slot, const double* in,
+                               double* out, double* energy, void* stream) {
+  AMA_REQUIRE(e && in && out, AMA_ERR_ARG, "null argument");
+  AMA_REQUIRE(slot >= 0 && slot < 4 && energy_slot >= -1 && energy_slot < 4, AMA_ERR_ARG, "bad slot");
+  auto it = g_filters.find(e);
+  AMA_REQUIRE(it != g_filters.end() && it->second.filt[slot], AMA_ERR_ARG, "filter slot not set");
+  const double* ef = nullptr;
+  if (energy_slot >= 0) {
+    ef = it->second.filt[energy_slot];
+    AMA_REQUIRE(ef && energy, AMA_ERR_ARG, "energy filter slot not set or energy is null");
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t need = (size_t)e->N * sizeof(double2);
+  if (g_grid_work_bytes < need) {
+    if (g_grid_work) cudaFree(g_grid_work);
+    g_grid_work = nullptr; g_grid_work_bytes = 0;
+    AMA_CUDA_TRY(cudaMalloc((void**)&g_grid_work, need));
+    g_grid_work_bytes = need;
+  }
+  GridView g = grid_view(e);
+  const size_t ps = plane_smem<double>(e), ss = slab_smem<double>(e);
+  static bool attrs = false;
+  if (!attrs) {
+    AMA_CUDA_TRY(cudaFuncSetAttribute(grid_g1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+    AMA_CUDA_TRY(cudaFuncSetAttribute(grid_g3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+    AMA_CUDA_TRY(cudaFuncSetAttribute(grid_g2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+    attrs = true;
+  }
+  auto T = [&](int axis, int dir) { return (const double2*)e->d.tw[AMA_C128][axis][dir]; };
+  const double invN = 1.0 / (double)e->N;
+  grid_g1_kernel<<<g.n1, kStageThreads, ps, s>>>(g, T(1, 1), T(2, 1), in, g_grid_work);
+  AMA_CHECK_LAUNCH();
+  grid_g2_kernel<<<g.n2, kStageThreads, ss, s>>>(g, T(0, 1), T(0, 0), it->second.filt[slot], ef, invN,
+                                                  invN * invN, g_grid_work, energy);
+  AMA_CHECK_LAUNCH();
+  grid_g3_kernel<<<g.n1, kStageThreads, ps, s>>>(g, T(1, 0), T(2, 0), g_grid_work, out);
+  AMA_CHECK_LAUNCH();
+  return AMA_OK;
+}

@@ -1,0 +1,163 @@
+// Complex GEMM on the SIMT pipes (FP32 or FP64), tiled 64x64 per CTA with a 4x4
+// complex micro-tile per thread, split-K over a partial-sum buffer for long reductions.
+//
+// Forms (all row-major):
+//   NN : C = alpha * A(m x k) * B(k x n)        + beta * C
+//   NC : C = alpha * A(m x k) * conj(B(n x k))^T + beta * C
+//   CN : C = alpha * conj(A(k x m))^T * B(k x n) + beta * C
+// Batches are described by a functor giving the matrix pointers and sizes of batch z,
+// which lets the engine run ragged per-k products (different npw per k) in one launch.
+#pragma once
+#include "common.cuh"
+
+namespace ama {
+
+enum GemmForm { kNN = 0, kNC = 1, kCN = 2 };
+
+template <typename C> struct GemmProblem {
+  const C* a; const C* b; C* c;
+  int m, n, k;
+  int64_t lda, ldb, ldc;
+};
+
+constexpr int kBM = 64, kBN = 64, kGemmThreads = 256;
+template <typename T> struct GemmBK { static constexpr int value = 16; };
+template <> struct GemmBK<double> { static constexpr int value = 8; };
+
+// One CTA computes a kBM x kBN tile of batch blockIdx.z / splits, reduction slice
+// blockIdx.z % splits. If `partial` is non-null the raw tile sum goes to
+// partial[(z_split * M*N ...)] (see engine), else the alpha/beta epilogue is applied.
+template <typename T, int FORM, class Batch>
+__global__ void __launch_bounds__(kGemmThreads)
+cgemm_tile_kernel(Batch batch, int splits, cx_t<T> alpha, cx_t<T> beta, cx_t<T>* partial,
+                  int64_t partial_stride) {
+  using C = cx_t<T>;
+  constexpr int BK = GemmBK<T>::value;
+  __shared__ C As[BK][kBM + 1];
+  __shared__ C Bs[BK][kBN + 1];
+
+  const int z = blockIdx.z;
+  const int bz = z / splits, sz = z % splits;
+  const GemmProblem<C> p = batch(bz);
+  const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * kBN;
+  if (m0 >= p.m || n0 >= p.n) return;
+  const int kchunk = ((p.k + splits - 1) / splits + BK - 1) / BK * BK;
+  const int kbeg = sz * kchunk;
+  const int kend = min(p.k, kbeg + kchunk);
+
+  const int tid = threadIdx.x;
+  const int tx = tid % 16, ty = tid / 16;
+  C acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = mk<C>(0, 0);
+
+  for (int k0 = kbeg; k0 < kend; k0 += BK) {
+    // ---- A tile -> As[kk][mm]
+    for (int e = tid; e < BK * kBM; e += kGemmThreads) {
+      int mm, kk;
+      if (FORM == kCN) { mm = e % kBM; kk = e / kBM; }   // A is (k x m): m contiguous
+      else { kk = e % BK; mm = e / BK; }                  // A is (m x k): k contiguous
+      const int gm = m0 + mm, gk = k0 + kk;
+      C v = mk<C>(0, 0);
+      if (gm < p.m && gk < kend) {
+        if (FORM == kCN) { v = p.a[(int64_t)gk * p.lda + gm]; v.y = -v.y; }
+        else v = p.a[(int64_t)gm * p.lda + gk];
+      }
+      As[kk][mm] = v;
+    }
+    // ---- B tile -> Bs[kk][nn]
+    for (int e = tid; e < BK * kBN; e += kGemmThreads) {
+      int nn, kk;
+      if (FORM == kNC) { kk = e % BK; nn = e / BK; }      // B is (n x k): k contiguous
+      else { nn = e % kBN; kk = e / kBN; }                // B is (k x n): n contiguous
+      const int gn = n0 + nn, gk = k0 + kk;
+      C v = mk<C>(0, 0);
+      if (gn < p.n && gk < kend) {
+        if (FORM == kNC) { v = p.b[(int64_t)gn * p.ldb + gk]; v.y = -v.y; }
+        else v = p.b[(int64_t)gk * p.ldb + gn];
+      }
+      Bs[kk][nn] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < BK; ++kk) {
+      C a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[kk][ty + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          acc[i][j].x += a[i].x * b[j].x - a[i].y * b[j].y;
+          acc[i][j].y += a[i].x * b[j].y + a[i].y * b[j].x;
+        }
+    }
+    __syncthreads();
+  }
+
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int gm = m0 + ty + 16 * i;
+    if (gm >= p.m) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int gn = n0 + tx + 16 * j;
+      if (gn >= p.n) continue;
+      if (partial) {
+        partial[(int64_t)z * partial_stride + (int64_t)gm * p.n + gn] = acc[i][j];
+      } else {
+        C* dst = p.c + (int64_t)gm * p.ldc + gn;
+        C r = cmul(alpha, acc[i][j]);
+        if (beta.x != T(0) || beta.y != T(0)) r = cadd(r, cmul(beta, *dst));
+        *dst = r;
+      }
+    }
+  }
+}
+
+// Sum the split-K partials of each batch and apply the epilogue.
+template <typename T, class Batch>
+__global__ void cgemm_reduce_kernel(Batch batch, int splits, cx_t<T> alpha, cx_t<T> beta,
+                                    const cx_t<T>* partial, int64_t partial_stride) {
+  using C = cx_t<T>;
+  const int bz = blockIdx.y;
+  const GemmProblem<C> p = batch(bz);
+  const int64_t total = (int64_t)p.m * p.n;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    C s = mk<C>(0, 0);
+    for (int sidx = 0; sidx < splits; ++sidx)
+      s = cadd(s, partial[(int64_t)(bz * splits + sidx) * partial_stride + e]);
+    const int gm = (int)(e / p.n), gn = (int)(e % p.n);
+    C* dst = p.c + (int64_t)gm * p.ldc + gn;
+    C r = cmul(alpha, s);
+    if (beta.x != T(0) || beta.y != T(0)) r = cadd(r, cmul(beta, *dst));
+    *dst = r;
+  }
+}
+
+// Launch helper. `max_m/max_n/max_k` bound the batch's sizes (grid shape); `splits` > 1
+// needs `partial` sized batch*splits*partial_stride elements with partial_stride >= m*n.
+template <typename T, int FORM, class Batch>
+cudaError_t launch_cgemm(Batch batch, int nbatch, int max_m, int max_n, int splits,
+                         cx_t<T> alpha, cx_t<T> beta, cx_t<T>* partial, int64_t partial_stride,
+                         cudaStream_t stream) {
+  dim3 grid((max_n + kBN - 1) / kBN, (max_m + kBM - 1) / kBM, nbatch * splits);
+  if (splits <= 1) {
+    cgemm_tile_kernel<T, FORM><<<grid, kGemmThreads, 0, stream>>>(batch, 1, alpha, beta, nullptr, 0);
+    return cudaGetLastError();
+  }
+  cgemm_tile_kernel<T, FORM><<<grid, kGemmThreads, 0, stream>>>(batch, splits, alpha, beta, partial,
+                                                                partial_stride);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  dim3 rgrid(64, nbatch);
+  cgemm_reduce_kernel<T><<<rgrid, 256, 0, stream>>>(batch, splits, alpha, beta, partial, partial_stride);
+  return cudaGetLastError();
+}
+
+}  // namespace ama

@@ -1,0 +1,69 @@
+// ama_zgemm: strided-batched complex GEMM for the Davidson subspace products.
+#include "common.cuh"
+#include "gemm.cuh"
+
+#include <algorithm>
+
+using namespace ama;
+
+namespace {
+
+template <typename C> struct StridedBatch {
+  const C* a; const C* b; C* c;
+  int m, n, k;
+  int64_t lda, ldb, ldc, sa, sb, sc;
+  __device__ GemmProblem<C> operator()(int z) const {
+    GemmProblem<C> p;
+    p.a = a + z * sa; p.b = b + z * sb; p.c = c + z * sc;
+    p.m = m; p.n = n; p.k = k; p.lda = lda; p.ldb = ldb; p.ldc = ldc;
+    return p;
+  }
+};
+
+struct Scratch { void* ptr = nullptr; size_t bytes = 0; };
+thread_local Scratch g_partial;
+
+template <typename T>
+int zgemm_impl(int form, int m, int n, int k, const double* alpha, const void* a, int64_t lda,
+               int64_t sa, const void* b, int64_t ldb, int64_t sb, const double* beta, void* c,
+               int64_t ldc, int64_t sc, int batch, cudaStream_t s) {
+  using C = cx_t<T>;
+  StridedBatch<C> sbch{(const C*)a, (const C*)b, (C*)c, m, n, k, lda, ldb, ldc, sa, sb, sc};
+  const C al = mk<C>(alpha[0], alpha[1]), be = mk<C>(beta[0], beta[1]);
+  const int tiles = ((m + kBM - 1) / kBM) * ((n + kBN - 1) / kBN) * batch;
+  int splits = std::max(1, std::min(32, (2 * 148 + tiles - 1) / tiles));
+  splits = std::min(splits, std::max(1, k / 512));
+  const int64_t pstride = (int64_t)m * n;
+  if (splits > 1) {
+    const size_t need = (size_t)batch * splits * pstride * sizeof(C);
+    if (g_partial.bytes < need) {
+      if (g_partial.ptr) cudaFree(g_partial.ptr);
+      g_partial.ptr = nullptr; g_partial.bytes = 0;
+      AMA_CUDA_TRY(cudaMalloc(&g_partial.ptr, need));
+      g_partial.bytes = need;
+    }
+  }
+  cudaError_t err;
+  if (form == 0) err = launch_cgemm<T, kNN>(sbch, batch, m, n, splits, al, be, (C*)g_partial.ptr, pstride, s);
+  else if (form == 1) err = launch_cgemm<T, kNC>(sbch, batch, m, n, splits, al, be, (C*)g_partial.ptr, pstride, s);
+  else err = launch_cgemm<T, kCN>(sbch, batch, m, n, splits, al, be, (C*)g_partial.ptr, pstride, s);
+  AMA_CUDA_TRY(err);
+  return AMA_OK;
+}
+
+}  // namespace
+
+extern "C" int ama_zgemm(int32_t precision, int32_t trans_b, int32_t m, int32_t n, int32_t k,
+                         const double* alpha, const void* a, int64_t lda, int64_t stride_a,
+                         const void* b, int64_t ldb, int64_t stride_b, const double* beta, void* c,
+                         int64_t ldc, int64_t stride_c, int32_t batch, void* stream) {
+  AMA_REQUIRE(precision == AMA_C64 || precision == AMA_C128, AMA_ERR_ARG, "bad precision");
+  AMA_REQUIRE(trans_b >= 0 && trans_b <= 2, AMA_ERR_ARG, "trans_b must be 0, 1 or 2");
+  AMA_REQUIRE(alpha && beta && a && b && c, AMA_ERR_ARG, "null argument");
+  AMA_REQUIRE(m >= 0 && n >= 0 && k >= 0 && batch >= 1, AMA_ERR_SHAPE, "negative size");
+  if (m == 0 || n == 0) return AMA_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  return precision == AMA_C64
+             ? zgemm_impl<float>(trans_b, m, n, k, alpha, a, lda, stride_a, b, ldb, stride_b, beta, c, ldc, stride_c, batch, s)
+             : zgemm_impl<double>(trans_b, m, n, k, alpha, a, lda, stride_a, b, ldb, stride_b, beta, c, ldc, stride_c, batch, s);
+}

@@ -1,0 +1,157 @@
+"""Device engine for one :class:`~amaterasu_b200.system.PlaneWaveSystem`.
+
+Owns the C-ABI handle (``AmaEngine``) that holds the sphere<->grid maps, kinetic
+energies, projector matrices and D.B in HBM, and exposes the batched device calls on
+torch tensors. Every call runs on torch's current CUDA stream.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import AMA_C64, AMA_C128, call
+
+PRECISIONS = {"complex64": AMA_C64, "complex128": AMA_C128, torch.complex64: AMA_C64,
+              torch.complex128: AMA_C128, np.complex64: AMA_C64, np.complex128: AMA_C128}
+TORCH_DTYPE = {AMA_C64: torch.complex64, AMA_C128: torch.complex128}
+
+
+def precision_code(p) -> int:
+    if isinstance(p, int) and p in (AMA_C64, AMA_C128):
+        return p
+    if isinstance(p, np.dtype):
+        p = p.type
+    try:
+        return PRECISIONS[p]
+    except KeyError:
+        raise ValueError(f"unsupported precision {p!r}; use complex64 or complex128") from None
+
+
+def require_cuda() -> torch.device:
+    if not torch.cuda.is_available():
+        raise RuntimeError("amaterasu_b200 needs a CUDA device (sm_100a); there is no CPU fallback")
+    return torch.device("cuda", torch.cuda.current_device())
+
+
+def stream_ptr() -> ct.c_void_p:
+    return ct.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def ptr(t: torch.Tensor) -> ct.c_void_p:
+    return ct.c_void_p(t.data_ptr())
+
+
+class DeviceEngine:
+    """The C-ABI engine of a system, plus per-k offsets for packed band blocks."""
+
+    def __init__(self, system, precisions=("complex128", "complex64")):
+        self.device = require_cuda()
+        lib = _lib.load()
+        self.system = system
+        spheres = system.wave_spheres
+        self.npw = np.array([len(s) for s in spheres], dtype=np.int32)
+        self.pw_off = np.concatenate([[0], np.cumsum(self.npw.astype(np.int64))])
+        self.nk = len(spheres)
+        self.grid_shape = tuple(int(n) for n in system.grid.shape)
+        self.N = int(np.prod(self.grid_shape))
+        self.nspin = system.nspin
+        miller = np.ascontiguousarray(np.concatenate([s.miller for s in spheres]).astype(np.int32))
+        kinetic = np.ascontiguousarray(np.concatenate([s.kinetic_energy for s in spheres]), dtype=np.float64)
+        self.kinetic = [torch.from_numpy(np.ascontiguousarray(s.kinetic_energy)).to(self.device)
+                        for s in spheres]
+        projs = system.projectors
+        self.nproj = 0 if projs[0] is None else len(projs[0])
+        if self.nproj:
+            pmat = np.ascontiguousarray(
+                np.concatenate([p.matrix.astype(np.complex128).ravel() for p in projs])).view(np.float64)
+            dij = np.ascontiguousarray(projs[0].dij, dtype=np.float64)
+        else:
+            pmat = np.zeros(2)
+            dij = np.zeros(1)
+        mask = 0
+        for p in precisions:
+            mask |= 1 << precision_code(p)
+        self.precisions = mask
+        desc = _lib.AmaSystemDesc(
+            n1=self.grid_shape[0], n2=self.grid_shape[1], n3=self.grid_shape[2], nk=self.nk,
+            npw=self.npw.ctypes.data_as(ct.POINTER(ct.c_int32)),
+            miller=miller.ctypes.data_as(ct.POINTER(ct.c_int32)),
+            kinetic=kinetic.ctypes.data_as(ct.POINTER(ct.c_double)),
+            nproj=self.nproj,
+            projectors=pmat.ctypes.data_as(ct.POINTER(ct.c_double)),
+            dij=dij.ctypes.data_as(ct.POINTER(ct.c_double)),
+            nspin=self.nspin, precisions=mask)
+        handle = ct.c_void_p()
+        with torch.cuda.device(self.device):
+            call("ama_engine_create", ct.byref(desc), ct.byref(handle))
+        self.handle = handle
+        self._lib = lib
+        self._potential_set = False
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            try:
+                self._lib.ama_engine_destroy(h)
+            except Exception:  # pragma: no cover - interpreter shutdown
+                pass
+            self.handle = None
+
+    def block_offsets(self, nbands: int, k_first: int = 0, k_count: int | None = None):
+        """Element offsets of each k's (nbands, npw_k) block in a packed all-k array."""
+        k_count = self.nk - k_first if k_count is None else k_count
+        sizes = self.npw[k_first:k_first + k_count].astype(np.int64) * nbands
+        return np.concatenate([[0], np.cumsum(sizes)])
+
+    def set_potential(self, v: torch.Tensor) -> None:
+        v = v.to(self.device, torch.float64).contiguous()
+        if v.shape != (self.nspin, *self.grid_shape):
+            raise ValueError(f"effective potential has shape {tuple(v.shape)}, "
+                             f"expected {(self.nspin, *self.grid_shape)}")
+        call("ama_set_potential", self.handle, ptr(v), self.nspin, stream_ptr())
+        self._v = v  # keep alive until the stream consumes it
+        self._potential_set = True
+
+    def reserve(self, precision, max_bands: int) -> None:
+        call("ama_reserve", self.handle, precision_code(precision), int(max_bands))
+
+    def hpsi(self, psi: torch.Tensor, out: torch.Tensor, *, k_first: int, k_count: int,
+             nbands: int, spin: int = 0) -> torch.Tensor:
+        prec = precision_code(psi.dtype)
+        expected = int(self.pw_off[k_first + k_count] - self.pw_off[k_first]) * nbands
+        if psi.numel() != expected or out.numel() != expected:
+            raise ValueError(f"packed psi has {psi.numel()} coefficients, expected {expected}")
+        call("ama_hpsi", self.handle, prec, k_first, k_count, nbands, spin, ptr(psi), ptr(out), stream_ptr())
+        return out
+
+    def density_accumulate(self, psi: torch.Tensor, weights: torch.Tensor, rho: torch.Tensor, *,
+                           k_first: int, k_count: int, nbands: int) -> None:
+        prec = precision_code(psi.dtype)
+        expected = int(self.pw_off[k_first + k_count] - self.pw_off[k_first]) * nbands
+        if psi.numel() != expected:
+            raise ValueError(f"packed psi has {psi.numel()} coefficients, expected {expected}")
+        if weights.dtype != torch.float64 or weights.numel() != k_count * nbands:
+            raise ValueError("weights must be float64 with k_count*nbands entries")
+        if rho.dtype != torch.float64 or rho.numel() != self.N:
+            raise ValueError("rho must be float64 with one value per grid point")
+        call("ama_density_accumulate", self.handle, prec, k_first, k_count, nbands, ptr(psi),
+             ptr(weights), ptr(rho), stream_ptr())
+
+    def project(self, psi: torch.Tensor, k: int) -> torch.Tensor:
+        prec = precision_code(psi.dtype)
+        nb = psi.shape[0]
+        out = torch.empty((nb, self.nproj), dtype=psi.dtype, device=psi.device)
+        call("ama_project", self.handle, prec, k, nb, ptr(psi), ptr(out), stream_ptr())
+        return out
+
+
+def engine_for(system, precisions=("complex128", "complex64")) -> DeviceEngine:
+    """The system's engine, created on first use and cached on the system object."""
+    eng = getattr(system, "_device_engine", None)
+    if eng is None:
+        eng = DeviceEngine(system, precisions)
+        system._device_engine = eng
+    return eng

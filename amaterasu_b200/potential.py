@@ -1,0 +1,107 @@
+"""Effective potential on the GPU in FP64: Hartree (reciprocal-space filter kernel),
+LDA-PZ exchange-correlation (pointwise kernel) and the local ionic potential.
+
+Mirrors amaterasu ``scf/driver.py:330-357`` (``effective_potential``),
+``hamiltonian/hartree.py:28-50`` and ``xc/driver.py:108-164`` (LDA branch: the
+unpolarised density is split n/2, n/2 and the spin-polarised functional evaluated).
+"""
+from __future__ import annotations
+
+import ctypes as ct
+
+import numpy as np
+import torch
+
+from ._lib import call
+from .engine import engine_for, ptr, stream_ptr
+
+HARTREE_SLOT = 0
+KERKER_SLOT = 1
+
+
+class GridOps:
+    """Grid-space FP64 operations of one system (cached on the system)."""
+
+    def __init__(self, system):
+        self.system = system
+        self.engine = engine_for(system)
+        self.device = self.engine.device
+        grid = system.grid
+        self.shape = tuple(int(n) for n in grid.shape)
+        self.N = int(np.prod(self.shape))
+        self.dv = grid.cell_volume_per_point
+        self.volume = grid.volume
+        sphere = system.density_sphere
+        flat = grid.flat_indices(sphere)
+        f = np.zeros(self.N)
+        nz = sphere.g2 > 1e-12
+        f[flat[nz]] = 4.0 * np.pi / sphere.g2[nz]
+        call("ama_set_grid_filter", self.engine.handle, HARTREE_SLOT, f.ctypes.data_as(ct.c_void_p))
+        self._kerker_q0 = None
+        self._energy = torch.zeros(1, dtype=torch.float64, device=self.device)
+
+    def hartree(self, total: torch.Tensor):
+        """(E_H in Hartree as a 0-d device tensor, V_H(r) flat) for a total density."""
+        total = total.reshape(-1).to(self.device, torch.float64).contiguous()
+        out = torch.empty_like(total)
+        self._energy.zero_()
+        call("ama_grid_filter", self.engine.handle, HARTREE_SLOT, HARTREE_SLOT, ptr(total), ptr(out),
+             ptr(self._energy), stream_ptr())
+        return self._energy[0] * (0.5 * self.volume), out
+
+    def set_kerker(self, q0: float, uniform_factor: float = 0.0):
+        if self._kerker_q0 == (q0, uniform_factor):
+            return
+        g = self.system.grid.gvectors_cartesian()
+        g2 = np.einsum("...i,...i->...", g, g).ravel()
+        with np.errstate(invalid="ignore", divide="ignore"):
+            f = np.where(g2 > 1e-12, g2 / (g2 + q0**2), float(uniform_factor))
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        call("ama_set_grid_filter", self.engine.handle, KERKER_SLOT, f.ctypes.data_as(ct.c_void_p))
+        self._kerker_q0 = (q0, uniform_factor)
+
+    def kerker(self, field: torch.Tensor) -> torch.Tensor:
+        field = field.reshape(-1).to(self.device, torch.float64).contiguous()
+        out = torch.empty_like(field)
+        call("ama_grid_filter", self.engine.handle, KERKER_SLOT, -1, ptr(field), ptr(out), None,
+             stream_ptr())
+        return out
+
+    def lda(self, density: torch.Tensor):
+        """(E_xc device scalar, v_xc (nspin, N)) for density (nspin, N) in electrons/Bohr^3."""
+        d = density.reshape(density.shape[0], -1).to(self.device, torch.float64)
+        nspin = d.shape[0]
+        spin = torch.stack([0.5 * d[0], 0.5 * d[0]]) if nspin == 1 else d
+        spin = spin.contiguous()
+        eps = torch.empty(self.N, dtype=torch.float64, device=self.device)
+        vrho = torch.empty((2, self.N), dtype=torch.float64, device=self.device)
+        call("ama_lda_pz", ptr(spin), self.N, ptr(eps), ptr(vrho), stream_ptr())
+        energy = (eps * (spin[0] + spin[1])).sum() * self.dv
+        return energy, vrho[:nspin]
+
+
+def grid_ops(system) -> GridOps:
+    ops = getattr(system, "_grid_ops", None)
+    if ops is None:
+        ops = GridOps(system)
+        system._grid_ops = ops
+    return ops
+
+
+def effective_potential(system, density):
+    """(v_eff (nspin, n1, n2, n3) device FP64, E_Hartree, E_xc) for a density."""
+    ops = grid_ops(system)
+    d = density if isinstance(density, torch.Tensor) else torch.from_numpy(np.asarray(density, float))
+    d = d.to(ops.device, torch.float64).reshape(system.nspin, -1)
+    e_h, v_h = ops.hartree(d.sum(0))
+    xc_density = d
+    if system.core_density is not None:
+        core = torch.from_numpy(system.core_density.ravel()).to(ops.device)
+        xc_density = d + core[None, :] / system.nspin
+    e_xc, v_xc = ops.lda(xc_density)
+    vloc = getattr(system, "_v_local_dev", None)
+    if vloc is None:
+        vloc = torch.from_numpy(system.v_local.ravel()).to(ops.device)
+        system._v_local_dev = vloc
+    v = vloc[None, :] + v_h[None, :] + v_xc
+    return v.reshape(system.nspin, *ops.shape), float(e_h), float(e_xc)

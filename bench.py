@@ -1,0 +1,336 @@
+#!/usr/bin/env python
+"""H.psi throughput (bands/s) of the B200 plane-wave engine on the Si64 workload.
+
+Workload (one step): H.psi for 160 bands at each of 4 k-points (Gamma + 3 seeded random
+k) of the 64-atom simple-cubic Si supercell (a = 10.86 A, synthetic analytic
+norm-conserving dataset, ecut 40 Ry, 84^3 grid, ~37k plane waves, 256 projectors), all
+four k-points in one batched call, psi and V_eff resident in HBM. psi is
+orthonormalised seeded N(0,1)/(1+|k+G|^2/2) noise; V_eff is built from the superposed
+atomic density. The per-step working set (~1.7 GB) exceeds L2, so no flush is needed.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0). `--impl reference` times the CPU oracle (a numpy/scipy
+FP64 restatement of the reference's Hamiltonian.apply) on the host cores instead.
+Under torchrun each rank runs the same workload on its own GPU (k-point sets are
+independent; no collective on the data path) and the value is the total over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+WORKLOAD = "si64_hpsi"
+METRIC = "Hpsi bands/s (Si64 40 Ry 84^3, 4 k x 160 bands)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["complex64", "complex128"], default="complex64")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def build_system_for_bench():
+    from amaterasu_b200.cells import workload
+    from amaterasu_b200.pseudo import read_upf, write_synthetic_upf
+    from amaterasu_b200.system import build_system
+    with tempfile.TemporaryDirectory() as tmp:
+        pseudo = read_upf(write_synthetic_upf(Path(tmp) / "Si.upf"))
+    structure, ecut, kset, nbands = workload(WORKLOAD)
+    system = build_system(structure, {"Si": pseudo}, ecut, 4 * ecut, kpoints=kset, nbands=nbands)
+    return system, nbands
+
+
+def orthonormal_bands(npw, nbands, kinetic, seed):
+    """random_bands of the reference (scf/eigen/subspace.py:79-88): damped noise,
+    Cholesky-orthonormalised."""
+    import scipy.linalg as sla
+    rng = np.random.default_rng(seed)
+    block = (rng.normal(size=(nbands, npw)) + 1j * rng.normal(size=(nbands, npw))) / (1.0 + kinetic)
+    factor = sla.cholesky(block @ block.conj().T, lower=True)
+    return sla.solve_triangular(factor, block, lower=True)
+
+
+def algorithmic_bytes(system, nbands, itemsize):
+    """Per all-k H.psi launch: per band 2*npw*s + 4*N*s, per launch N*4 (V) and
+    nproj*npw*s per k (projectors)."""
+    N = int(np.prod(system.grid.shape))
+    nproj = len(system.projectors[0])
+    total = 0
+    for w in system.wave_spheres:
+        npw = len(w)
+        total += nbands * (2 * npw * itemsize + 4 * N * itemsize) + nproj * npw * itemsize
+    return total + N * 4
+
+
+class ClockSampler:
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def start(self):
+        def run():
+            q = ("--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap")
+            while not self._stop.is_set():
+                try:
+                    out = subprocess.run(["nvidia-smi", q, "--format=csv,noheader,nounits", "-i",
+                                          str(self.index)], capture_output=True, text=True, timeout=5)
+                    self.samples.append([x.strip() for x in out.stdout.strip().split(",")])
+                except Exception:
+                    pass
+                self._stop.wait(0.2)
+        self._t = threading.Thread(target=run, daemon=True)
+        self._t.start()
+
+    def stop(self):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if len(s) >= 6 and s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if len(s) >= 6 and s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples if len(s) >= 6
+                          for i in range(4) if s[2 + i].strip() == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+def cpu_hpsi_sample(system, veff, nbands_sample, seconds, threads):
+    """Time the oracle's FP64 H.psi on a bounded sample of the workload: blocks of
+    `nbands_sample` bands cycling over the k-points until `seconds` have passed."""
+    from threadpoolctl import threadpool_limits
+    from oracle.hamiltonian import hamiltonian_apply
+    blocks = []
+    for ik, w in enumerate(system.wave_spheres):
+        rng = np.random.default_rng(1000 + ik)
+        psi = (rng.normal(size=(nbands_sample, len(w))) + 1j * rng.normal(size=(nbands_sample, len(w))))
+        blocks.append(psi / (1.0 + w.kinetic_energy))
+    done = 0
+    t0 = time.perf_counter()
+    with threadpool_limits(limits=threads):
+        while True:
+            for ik, w in enumerate(system.wave_spheres):
+                p = system.projectors[ik]
+                hamiltonian_apply(blocks[ik], w.miller, system.grid.shape, w.kinetic_energy, veff,
+                                  p.matrix, p.dij, workers=threads)
+                done += nbands_sample
+            if time.perf_counter() - t0 > seconds:
+                break
+    elapsed = time.perf_counter() - t0
+    return done / elapsed, done, elapsed
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from amaterasu_b200.potential import effective_potential  # noqa: F401  (not used: CPU path)
+    from oracle.potential import hartree, xc_on_grid
+    system, nbands = build_system_for_bench()
+    rho0 = system.initial_density()
+    sph = system.density_sphere
+    _, v_h = hartree(rho0[0], system.grid.shape, sph.miller, sph.g2, system.grid.volume)
+    _, v_xc = xc_on_grid(rho0, system.grid.cell_volume_per_point)
+    veff = system.v_local + v_h + v_xc[0]
+    threads = os.cpu_count() or 1
+    per_step = []
+    sample_bands = 8
+    for step in range(args.warmup + args.steps):
+        rate, done, elapsed = cpu_hpsi_sample(system, veff, sample_bands, 0.0, threads)
+        if step >= args.warmup:
+            per_step.append((done, elapsed))
+    done = sum(d for d, _ in per_step)
+    elapsed = sum(e for _, e in per_step)
+    value = done / elapsed
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "bands/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * elapsed / max(args.steps, 1), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "complex128", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "cell": "Si64 sc a=10.86 A", "ecut_ry": 40,
+                   "grid": list(system.grid.shape), "kpoints": 4, "bands_per_k": nbands,
+                   "sample": f"{sample_bands} bands at each of the 4 k-points per step"},
+        "cpu_baseline": {"value": value, "unit": "bands/s", "cores": threads, "kind": "port",
+                         "sample": f"{sample_bands} bands x 4 k per step, oracle FP64 H.psi, "
+                                   f"scipy.fft workers={threads}, BLAS threads={threads}"},
+        "e2e": {"value": value, "unit": "bands/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+
+    from amaterasu_b200.engine import engine_for
+    from amaterasu_b200.hamiltonian import Hamiltonian
+    from amaterasu_b200.potential import effective_potential
+
+    system, nbands = build_system_for_bench()
+    nk = len(system.wave_spheres)
+    veff, _, _ = effective_potential(system, system.initial_density())
+    prec = args.precision
+    cdtype = torch.complex64 if prec == "complex64" else torch.complex128
+    itemsize = 8 if prec == "complex64" else 16
+    H = Hamiltonian(system, veff, precision=prec)
+    eng = engine_for(system)
+    blocks = [orthonormal_bands(len(w), nbands, w.kinetic_energy, 12345 + ik)
+              for ik, w in enumerate(system.wave_spheres)]
+    host = np.concatenate([b.ravel() for b in blocks]).astype(np.complex64 if prec == "complex64"
+                                                              else np.complex128)
+    psi = torch.from_numpy(host).cuda().to(cdtype)
+    out = torch.empty_like(psi)
+    eng.reserve(prec, nk * nbands)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        H.apply_all(psi, nbands, out=out)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(args.steps):
+        step()
+    stop.record(stream)
+    torch.cuda.synchronize()
+    ms = start.elapsed_time(stop)
+
+    # end-to-end through the public API: pinned host psi -> device, H.psi, device -> pinned host
+    pinned_in = torch.from_numpy(host).pin_memory()
+    pinned_out = torch.empty_like(pinned_in).pin_memory()
+    dev_in = torch.empty_like(psi)
+    for _ in range(2):
+        dev_in.copy_(pinned_in, non_blocking=True)
+        H.apply_all(dev_in, nbands, out=out)
+        pinned_out.copy_(out, non_blocking=True)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        dev_in.copy_(pinned_in, non_blocking=True)
+        H.apply_all(dev_in, nbands, out=out)
+        pinned_out.copy_(out, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    clocks = sampler.stop()
+
+    t = torch.tensor([ms, e2e_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms, e2e_ms = float(t[0]), float(t[1])
+    bands_step = nk * nbands
+    value = world * bands_step * args.steps / (ms / 1e3)
+    e2e_value = world * bands_step * args.steps / (e2e_ms / 1e3)
+
+    # second precision for the record (same workload, complex128)
+    extra = {}
+    if prec == "complex64":
+        H2 = Hamiltonian(system, veff, precision="complex128")
+        psi2 = torch.from_numpy(np.concatenate([b.ravel() for b in blocks])).cuda()
+        out2 = torch.empty_like(psi2)
+        for _ in range(3):
+            H2.apply_all(psi2, nbands, out=out2)
+        torch.cuda.synchronize()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        n2 = max(3, args.steps // 2)
+        a0.record(stream)
+        for _ in range(n2):
+            H2.apply_all(psi2, nbands, out=out2)
+        a1.record(stream)
+        torch.cuda.synchronize()
+        ms2 = a0.elapsed_time(a1) / n2
+        peak_c128 = algorithmic_bytes(system, nbands, 16) / (ms2 / 1e3) / 1e9
+        extra["complex128"] = {"value": bands_step / (ms2 / 1e3), "unit": "bands/s",
+                               "ms_per_step": ms2, "achieved_gbs": peak_c128}
+        del H2, psi2, out2
+
+    peaks = {}
+    try:
+        peaks = json.loads((REPO / "MEASURED_PEAKS.json").read_text())
+    except Exception:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    per_launch_s = ms / 1e3 / args.steps
+    alg = algorithmic_bytes(system, nbands, itemsize)
+    achieved = alg / per_launch_s / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": "bands/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c64" if prec == "complex64" else "c128",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "cell": "Si64 sc a=10.86 A, synthetic NC dataset",
+                   "ecut_ry": 40, "grid": list(system.grid.shape),
+                   "npw": [len(w) for w in system.wave_spheres], "nproj": len(system.projectors[0]),
+                   "kpoints": nk, "bands_per_k": nbands, "batched": "all k in one call",
+                   "l2": "working set > L2 (no flush)", "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "what": "whole H.psi call (stages A/B/C + projector GEMMs), algorithmic bytes",
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback"},
+        "e2e": {"value": e2e_value, "unit": "bands/s",
+                "h2d_bytes_per_step": int(host.nbytes), "d2h_bytes_per_step": int(host.nbytes)},
+        "gpu_launches": args.steps * 6,
+        "clocks": clocks,
+        **extra,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle.potential import hartree, xc_on_grid  # noqa: F401
+        veff_np = veff[0].cpu().numpy()
+        rate, done, elapsed = cpu_hpsi_sample(system, veff_np, 4, 10.0, 1)
+        line["cpu_baseline"] = {"value": rate, "unit": "bands/s", "cores": 1, "kind": "port",
+                                "sample": f"{done} bands (4-band blocks cycling over the 4 k-points, "
+                                          f"{elapsed:.1f} s), oracle FP64 H.psi, scipy.fft workers=1, BLAS 1 thread"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,143 @@
+/*
+ * amaterasu_b200 C-ABI: a B200 (sm_100a) plane-wave Kohn-Sham engine.
+ *
+ * Every entry point returns an int status (AMA_OK or an AMA_ERR_* code); the message of
+ * the last failure on the calling thread is returned by ama_last_error(). Array
+ * arguments are plain pointers: "host" arrays are read before the call returns, "device"
+ * arrays are CUDA device pointers that the call uses in stream order on `stream`
+ * (a cudaStream_t passed as void*; NULL means the legacy default stream). Complex arrays
+ * are interleaved (re, im) pairs of float (AMA_C64) or double (AMA_C128).
+ *
+ * The entry points replace the numpy routines of the reference Python package
+ * (amaterasu 0.1.0a2); each declaration names the reference function it stands in for.
+ * One engine per stream; engines share no mutable state.
+ */
+#ifndef AMA_H_
+#define AMA_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define AMA_API __attribute__((visibility("default")))
+#else
+#define AMA_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  AMA_OK = 0,
+  AMA_ERR_SHAPE = 1,         /* shape/size mismatch (Python: ValueError)            */
+  AMA_ERR_CUDA = 2,          /* a CUDA runtime or library call failed               */
+  AMA_ERR_NOT_CONVERGED = 3, /* an iteration hit its limit                          */
+  AMA_ERR_TIMEOUT = 4,       /* a bounded device wait ran out                       */
+  AMA_ERR_NOT_SPD = 5,       /* Cholesky met a non-positive pivot                   */
+  AMA_ERR_ARG = 6,           /* invalid argument (null pointer, bad enum)           */
+  AMA_ERR_UNSUPPORTED = 7    /* a size or option the engine does not implement      */
+};
+
+enum { AMA_C64 = 0, AMA_C128 = 1 };
+
+typedef struct AmaEngine AmaEngine;
+
+typedef struct AmaSystemDesc {
+  int32_t n1, n2, n3;        /* FFT grid, C order (axis 2 fastest)                   */
+  int32_t nk;                /* number of k-points                                   */
+  const int32_t* npw;        /* host [nk]: plane waves per k                          */
+  const int32_t* miller;     /* host [sum npw][3]: Miller indices, sphere order, k-major */
+  const double* kinetic;     /* host [sum npw]: |k+G|^2/2 in Hartree                  */
+  int32_t nproj;             /* projector rows (same for every k), may be 0           */
+  const double* projectors;  /* host complex [sum_k nproj*npw_k]: <k+G|beta_i>, k-major,
+                                row-major (nproj, npw_k) per k; may be NULL if nproj==0 */
+  const double* dij;         /* host [nproj*nproj]: D_ij in Hartree                   */
+  int32_t nspin;             /* 1 or 2                                               */
+  uint32_t precisions;       /* bit AMA_C64: keep complex64 copies; bit AMA_C128: complex128 */
+} AmaSystemDesc;
+
+AMA_API const char* ama_last_error(void);
+AMA_API int ama_version(void);
+
+/* Build an engine: index maps, kinetic energies, projector matrices and D.B on the
+ * current CUDA device. Replaces the per-geometry tables the reference builds in
+ * hamiltonian/system.py:215-379 (wave spheres, fft.py:174-190 indices, kb.py:260-343). */
+AMA_API int ama_engine_create(const AmaSystemDesc* desc, AmaEngine** engine);
+AMA_API int ama_engine_destroy(AmaEngine* engine);
+
+/* Effective potential V_eff(r) for each spin channel, device FP64 [nspin][n1*n2*n3],
+ * natural grid order. Replaces Hamiltonian.__init__ (hamiltonian/operator.py:49-58). */
+AMA_API int ama_set_potential(AmaEngine* engine, const double* v, int32_t nspin, void* stream);
+
+/* Pre-size the H.psi workspace for up to `max_bands` bands in flight (sum over the
+ * k-points of one call). Optional: ama_hpsi grows it on demand. */
+AMA_API int ama_reserve(AmaEngine* engine, int32_t precision, int64_t max_bands);
+
+/* H.psi = T psi + G[V R[psi]] + B^H D B psi for `nbands` bands at each of the k-points
+ * k_first .. k_first+k_count-1. psi/hpsi are device arrays holding, back to back, one
+ * row-major (nbands, npw_k) block per k-point. Replaces Hamiltonian.apply
+ * (hamiltonian/operator.py:60-69) batched over k. */
+AMA_API int ama_hpsi(AmaEngine* engine, int32_t precision, int32_t k_first, int32_t k_count,
+             int32_t nbands, int32_t spin, const void* psi, void* hpsi, void* stream);
+
+/* Occupation-weighted density: rho[spin][r] += sum_k sum_n weights[k*nbands+n] |u_nk(r)|^2
+ * over the bands of k_first..k_first+k_count-1 (device weights, FP64), accumulated in
+ * FP64 into the device array rho [n1*n2*n3] (natural order; caller zeroes it and applies
+ * 1/Omega). Replaces the inner loop of compute_density (scf/density.py:60-71). */
+AMA_API int ama_density_accumulate(AmaEngine* engine, int32_t precision, int32_t k_first,
+                           int32_t k_count, int32_t nbands, const void* psi,
+                           const double* weights, double* rho, void* stream);
+
+/* <beta_i|psi_n> for one k-point: proj[n][i] = sum_G psi[n][G] conj(B[i][G]).
+ * Replaces KBProjectors.project (pseudo/kb.py:216-218). */
+AMA_API int ama_project(AmaEngine* engine, int32_t precision, int32_t k, int32_t nbands,
+                const void* psi, void* proj, void* stream);
+
+/* Complex GEMM on device arrays, batched with fixed strides:
+ *   trans_b == 0: C[b] = alpha * A[b] (m x k) * B[b] (k x n)           + beta * C[b]
+ *   trans_b == 1: C[b] = alpha * A[b] (m x k) * conj(B[b] (n x k))^T   + beta * C[b]
+ *   trans_b == 2: C[b] = alpha * conj(A[b] (k x m))^T * B[b] (k x n)   + beta * C[b]
+ * All matrices row-major with leading dimensions lda/ldb/ldc (elements); alpha and beta
+ * are complex (re, im) in double. Replaces the ndarray products of the Davidson
+ * subspace steps (scf/eigen/subspace.py:24-76, davidson.py:81-100). */
+AMA_API int ama_zgemm(int32_t precision, int32_t trans_b, int32_t m, int32_t n, int32_t k,
+              const double* alpha, const void* a, int64_t lda, int64_t stride_a,
+              const void* b, int64_t ldb, int64_t stride_b, const double* beta, void* c,
+              int64_t ldc, int64_t stride_c, int32_t batch, void* stream);
+
+/* Teter-Payne-Allan preconditioning fused with the residual and normalisation:
+ *   r = hx - eps*x; t_n = sum_G |x|^2 T_G; out = K(T_G / max(t_n,1e-8)) r / ||.||
+ * for the `nrows` rows listed in `rows` (device int32); norms (device FP64 [nbands]) get
+ * ||hx - eps x|| for every band. Replaces davidson.py:81-93 and precond.py:27-46. */
+AMA_API int ama_residual_precondition(int32_t precision, int32_t nbands, int32_t npw,
+                              const void* x, const void* hx, const double* eps,
+                              const double* kinetic, double* norms, const int32_t* rows,
+                              int32_t nrows, void* out, void* stream);
+
+/* Reciprocal-space filter of a real grid field (FP64): stores a filter f(G) (host array,
+ * natural FFT order, one value per grid point) in slot 0..3 of the engine. */
+AMA_API int ama_set_grid_filter(AmaEngine* engine, int32_t slot, const double* filter);
+
+/* out(r) = Re sum_G f_slot(G) rho(G) e^{iG.r} with rho(G) = (1/N) sum_r rho(r) e^{-iG.r}
+ * (device FP64 arrays [n1*n2*n3], natural order); if energy_slot >= 0, *energy (device
+ * double) += sum_G f_energy_slot(G) |rho(G)|^2. With f = 4pi/G^2 on the density sphere this
+ * is the Hartree potential and energy (hamiltonian/hartree.py:28-50); with
+ * f = G^2/(G^2+q0^2) the Kerker filter (scf/mixing.py:94-105). */
+AMA_API int ama_grid_filter(AmaEngine* engine, int32_t slot, int32_t energy_slot,
+                            const double* in, double* out, double* energy, void* stream);
+
+/* LDA exchange plus Perdew-Zunger 1981 correlation on a spin-resolved density
+ * (device FP64, rho [2][npoints]); writes eps_xc [npoints] and v_xc [2][npoints].
+ * Replaces lda.exchange + lda.correlation_pz81 (xc/lda.py:122-142,203-262). */
+AMA_API int ama_lda_pz(const double* rho, int64_t npoints, double* eps, double* vrho, void* stream);
+
+/* Dense FP64 Hermitian eigensolver for `batch` matrices of order n (device, row-major,
+ * interleaved complex, overwritten by eigenvectors as columns); eigenvalues ascending.
+ * Replaces scipy.linalg.eigh in rayleigh_ritz (scf/eigen/subspace.py:74). */
+AMA_API int ama_heev(int32_t n, void* matrices, double* eigenvalues, int32_t batch, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AMA_H_ */
