@@ -1,0 +1,89 @@
+"""The subset of the reference's configuration schema the SCF path reads.
+
+Field names, defaults and units follow amaterasu ``config/schema.py:50-388``
+(XCConfig, KpointsConfig, OccupationsConfig (smearing in eV), MixingConfig, SCFConfig).
+An ``EngineConfig`` section holds the options of this engine that the reference does not
+have (working precision policy, batching); it is kept separate from the reference schema.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+
+@dataclass
+class XCConfig:
+    functional: str = "LDA-PZ"
+
+
+@dataclass
+class KpointsConfig:
+    scheme: str = "monkhorst-pack"
+    grid: list = field(default_factory=lambda: [1, 1, 1])
+    shift: list = field(default_factory=lambda: [0.0, 0.0, 0.0])
+    points: list | None = None
+    weights: list | None = None
+    symmetry: bool = False
+
+
+@dataclass
+class OccupationsConfig:
+    scheme: str = "gaussian"
+    smearing: float = 0.05          # eV unless given as "<value> Ha" / "<value> Ry"
+    order: int = 1
+    nbands: int | None = None
+
+
+@dataclass
+class MixingConfig:
+    algorithm: str = "pulay"
+    beta: float = 0.4
+    history: int = 8
+    preconditioner: str = "kerker"
+    kerker_q0: float = 1.5
+
+
+@dataclass
+class SCFConfig:
+    method: str = "mixing"
+    eigensolver: str = "davidson"
+    mixing: MixingConfig = field(default_factory=MixingConfig)
+    max_steps: int = 100
+    tol_energy: float = 1e-6        # eV per atom
+    tol_density: float = 1e-7       # integrated |dn| per electron
+
+
+@dataclass
+class EngineConfig:
+    """Engine-only options.
+
+    ``precision``: "complex128" (plain FP64), "complex64", or "mixed" (complex64 bulk,
+    complex128 once the density residual drops below ``refine_below``).
+    """
+    precision: str = "complex128"
+    refine_below: float = 1e-6
+    batched: bool = True
+
+
+@dataclass
+class Config:
+    xc: XCConfig = field(default_factory=XCConfig)
+    kpoints: KpointsConfig = field(default_factory=KpointsConfig)
+    occupations: OccupationsConfig = field(default_factory=OccupationsConfig)
+    scf: SCFConfig = field(default_factory=SCFConfig)
+    engine: EngineConfig = field(default_factory=EngineConfig)
+
+
+def parse_energy(value, default_unit: str = "eV") -> float:
+    """Energy in Hartree from a number (in ``default_unit``) or a '<value> <unit>' string."""
+    from .units import EV_IN_HARTREE, RYDBERG_IN_HARTREE
+    units = {"ha": 1.0, "hartree": 1.0, "au": 1.0, "ry": RYDBERG_IN_HARTREE, "ryd": RYDBERG_IN_HARTREE,
+             "rydberg": RYDBERG_IN_HARTREE, "ev": EV_IN_HARTREE}
+    if isinstance(value, str):
+        parts = value.strip().split()
+        number = float(parts[0])
+        unit = parts[1].lower() if len(parts) > 1 else default_unit.lower()
+    else:
+        number, unit = float(value), default_unit.lower()
+    if unit not in units:
+        raise ValueError(f"unknown energy unit {unit!r}")
+    return number * units[unit]

@@ -885,6 +885,35 @@ __global__ void grid_g3_kernel(GridView g, const double2* tw_y, const double2* t
 
 }  // namespace
 
+namespace {
+// Forward x transform of the G1 output and scatter to natural (x, y, z) order with 1/N:
+// out[G] = (1/N) sum_r in(r) e^{-iG.r}.
+__global__ void grid_g2f_kernel(GridView g, const double2* tw_f, const double2* __restrict__ work,
+                                double2* __restrict__ out, double scale) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* slab = reinterpret_cast<double2*>(smem_raw);
+  double2* twf = slab + (int64_t)g.n1 * g.n3;
+  const int p2 = blockIdx.x;
+  load_twiddles(twf, tw_f, g.n1);
+  const double2* wb = work + (int64_t)p2 * g.n3;
+  const int total = g.n1 * g.n3;
+  for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    const int x = e / g.n3, z = e % g.n3;
+    slab[e] = wb[(int64_t)x * g.plane_elems + z];
+  }
+  __syncthreads();
+  dft_cols<-1, true>(slab, g.n1, g.A1, g.B1, g.n3, twf);
+  const int y = p2 / g.B2 + g.A2 * (p2 % g.B2);
+  for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    const int p1 = e / g.n3, p3 = e % g.n3;
+    const int x = p1 / g.B1 + g.A1 * (p1 % g.B1);
+    const int z = p3 / g.B3 + g.A3 * (p3 % g.B3);
+    const double2 c = slab[e];
+    out[((int64_t)x * g.n2 + y) * g.n3 + z] = make_double2(c.x * scale, c.y * scale);
+  }
+}
+}  // namespace
+
 struct AmaGridFilters {
   double* filt[4] = {};
 };
@@ -943,13 +972,9 @@ extern "C" int ama_grid_filter(AmaEngine* e, int32_t slot, int32_t energy_slot, 
   }
   GridView g = grid_view(e);
   const size_t ps = plane_smem<double>(e), ss = slab_smem<double>(e);
-  static bool attrs = false;
-  if (!attrs) {
-    AMA_CUDA_TRY(cudaFuncSetAttribute(grid_g1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-    AMA_CUDA_TRY(cudaFuncSetAttribute(grid_g3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-    AMA_CUDA_TRY(cudaFuncSetAttribute(grid_g2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-    attrs = true;
-  }
+  AMA_CUDA_TRY(cudaFuncSetAttribute(grid_g1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
+  AMA_CUDA_TRY(cudaFuncSetAttribute(grid_g3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
+  AMA_CUDA_TRY(cudaFuncSetAttribute(grid_g2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
   auto T = [&](int axis, int dir) { return (const double2*)e->d.tw[AMA_C128][axis][dir]; };
   const double invN = 1.0 / (double)e->N;
   grid_g1_kernel<<<g.n1, kStageThreads, ps, s>>>(g, T(1, 1), T(2, 1), in, g_grid_work);
@@ -958,6 +983,29 @@ extern "C" int ama_grid_filter(AmaEngine* e, int32_t slot, int32_t energy_slot, 
                                                   invN * invN, g_grid_work, energy);
   AMA_CHECK_LAUNCH();
   grid_g3_kernel<<<g.n1, kStageThreads, ps, s>>>(g, T(1, 0), T(2, 0), g_grid_work, out);
+  AMA_CHECK_LAUNCH();
+  return AMA_OK;
+}
+
+extern "C" int ama_grid_fft_forward(AmaEngine* e, const double* in, void* out, void* stream) {
+  AMA_REQUIRE(e && in && out, AMA_ERR_ARG, "null argument");
+  AMA_REQUIRE(e->precisions & (1u << AMA_C128), AMA_ERR_ARG, "grid transforms need the complex128 tables");
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t need = (size_t)e->N * sizeof(double2);
+  if (g_grid_work_bytes < need) {
+    if (g_grid_work) cudaFree(g_grid_work);
+    g_grid_work = nullptr; g_grid_work_bytes = 0;
+    AMA_CUDA_TRY(cudaMalloc((void**)&g_grid_work, need));
+    g_grid_work_bytes = need;
+  }
+  GridView g = grid_view(e);
+  const size_t ps = plane_smem<double>(e), ss = slab_smem<double>(e);
+  AMA_CUDA_TRY(cudaFuncSetAttribute(grid_g1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
+  AMA_CUDA_TRY(cudaFuncSetAttribute(grid_g2f_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
+  auto T = [&](int axis, int dir) { return (const double2*)e->d.tw[AMA_C128][axis][dir]; };
+  grid_g1_kernel<<<g.n1, kStageThreads, ps, s>>>(g, T(1, 1), T(2, 1), in, g_grid_work);
+  AMA_CHECK_LAUNCH();
+  grid_g2f_kernel<<<g.n2, kStageThreads, ss, s>>>(g, T(0, 1), g_grid_work, (double2*)out, 1.0 / (double)e->N);
   AMA_CHECK_LAUNCH();
   return AMA_OK;
 }

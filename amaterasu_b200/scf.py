@@ -1,0 +1,246 @@
+"""The self-consistent field loop on the GPU (norm-conserving, symmetry off).
+
+Mirrors amaterasu ``scf/driver.py:372-569`` (``run_scf``, mixing branch): per iteration
+v_eff[n_in] (Hartree + LDA + local), Davidson at every (spin, k) with the tolerance
+schedule clip(1e-3 min(residual, 1), 1e-11, 1e-6) and 40/20 iterations, occupations,
+n_out, the Kohn-Sham energy at n_out, the eigenvalue-sum identity, the density residual
+integral |n_out - n_in| / N_e, convergence when |dF| < tol_energy * natoms (eV -> Ha) and
+the residual < tol_density (from the second iteration on), then mixing. Starting
+orbitals are random_bands seeded 12345 + 991 spin + ik (driver.py:360-369).
+
+Precision policy (``config.engine.precision``): "complex128" is the plain FP64 engine;
+"mixed" runs H.psi, Davidson and the density in complex64 and switches the orbitals to
+complex128 once the density residual falls below ``refine_below``, so the fixed point is
+the FP64 one. Energies, densities, potentials and subspace eigensolves are FP64 always.
+"""
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from .config import Config, parse_energy
+from .density import accumulate_packed, band_weights, finalize_density
+from .eigen import davidson, random_bands
+from .engine import engine_for, require_cuda
+from .hamiltonian import Hamiltonian
+from .mixing import create_mixer
+from .occupations import compute_occupations
+from .potential import effective_potential, grid_ops
+from .units import EV_IN_HARTREE, HARTREE_IN_EV
+
+__all__ = ["Energies", "SCFResult", "run_scf"]
+
+
+@dataclass
+class Energies:
+    kinetic: float = 0.0
+    local: float = 0.0
+    hartree: float = 0.0
+    xc: float = 0.0
+    nonlocal_: float = 0.0
+    ewald: float = 0.0
+    entropy: float = 0.0
+
+    @property
+    def total(self) -> float:
+        return self.kinetic + self.local + self.hartree + self.xc + self.nonlocal_ + self.ewald
+
+    @property
+    def free_energy(self) -> float:
+        return self.total - self.entropy
+
+    @property
+    def extrapolated(self) -> float:
+        return self.total - 0.5 * self.entropy
+
+
+@dataclass
+class SCFResult:
+    converged: bool
+    iterations: int
+    energies: Energies
+    eigenvalues: np.ndarray
+    occupations: np.ndarray
+    fermi_level: float
+    gap: float | None
+    magnetization: float
+    density: np.ndarray
+    wavefunctions: list
+    history: list = field(default_factory=list)
+    electron_count: float = 0.0
+    seconds: float = 0.0
+    precision_trace: list = field(default_factory=list)
+    seconds_per_iteration: list = field(default_factory=list)
+
+
+class _Orbitals:
+    """All (spin, k) orbital blocks in one packed device buffer per spin."""
+
+    def __init__(self, system, nbands, dtype, device):
+        self.system = system
+        self.nbands = nbands
+        self.eng = engine_for(system)
+        self.offsets = self.eng.block_offsets(nbands)
+        self.dtype = dtype
+        total = int(self.offsets[-1])
+        self.packed = [torch.empty(total, dtype=dtype, device=device) for _ in range(system.nspin)]
+
+    def block(self, spin, ik) -> torch.Tensor:
+        a, b = int(self.offsets[ik]), int(self.offsets[ik + 1])
+        return self.packed[spin][a:b].view(self.nbands, -1)
+
+    def set(self, spin, ik, value):
+        self.block(spin, ik).copy_(value)
+
+    def to(self, dtype):
+        self.packed = [p.to(dtype) for p in self.packed]
+        self.dtype = dtype
+
+
+def _kinetic_energy(system, orb: _Orbitals, occ, kin_dev) -> float:
+    g = 2.0 / system.nspin
+    total = torch.zeros((), dtype=torch.float64, device=orb.packed[0].device)
+    for spin in range(system.nspin):
+        for ik in range(system.nkpoints):
+            x = orb.block(spin, ik)
+            per_band = (x.real.double() ** 2 + x.imag.double() ** 2) @ kin_dev[ik]
+            f = torch.from_numpy(g * system.kpoints.weights[ik] * occ[spin, ik]).to(per_band.device)
+            total = total + (f * per_band).sum()
+    return float(total)
+
+
+def _nonlocal_energy(system, orb: _Orbitals, occ, dij_dev) -> float:
+    eng = orb.eng
+    if eng.nproj == 0:
+        return 0.0
+    g = 2.0 / system.nspin
+    total = torch.zeros((), dtype=torch.float64, device=orb.packed[0].device)
+    for spin in range(system.nspin):
+        for ik in range(system.nkpoints):
+            p = eng.project(orb.block(spin, ik), ik).to(torch.complex128)
+            quad = torch.einsum("ni,ij,nj->n", p.conj(), dij_dev, p).real
+            f = torch.from_numpy(g * system.kpoints.weights[ik] * occ[spin, ik]).to(quad.device)
+            total = total + (f * quad).sum()
+    return float(total)
+
+
+def _density_out(system, orb: _Orbitals, occ) -> torch.Tensor:
+    rho = torch.zeros((system.nspin, orb.eng.N), dtype=torch.float64, device=orb.packed[0].device)
+    for spin in range(system.nspin):
+        accumulate_packed(system, orb.packed[spin], orb.nbands, band_weights(system, occ, spin), rho[spin])
+    return finalize_density(system, rho)
+
+
+def run_scf(system, config: Config | None = None, *, logger=None, wavefunctions=None, density=None) -> SCFResult:
+    """Run the SCF loop to self-consistency on the GPU."""
+    config = config or Config()
+    if config.scf.method != "mixing":
+        raise NotImplementedError(f"scf.method {config.scf.method!r}: only density mixing is implemented")
+    log = logger or (lambda *_: None)
+    dev = require_cuda()
+    started = time.perf_counter()
+    natoms = system.natoms
+    smearing = 0.0 if config.occupations.scheme == "fixed" else parse_energy(config.occupations.smearing, "eV")
+    policy = config.engine.precision
+    wdtype = torch.complex64 if policy in ("mixed", "complex64") else torch.complex128
+    nb = system.nbands
+    eng = engine_for(system)
+    ops = grid_ops(system)
+    N = eng.N
+    dv = system.grid.cell_volume_per_point
+
+    if density is None:
+        rho_in = torch.from_numpy(system.initial_density().reshape(system.nspin, -1)).to(dev)
+    else:
+        d = density if isinstance(density, torch.Tensor) else torch.from_numpy(np.asarray(density, float))
+        rho_in = d.to(dev, torch.float64).reshape(system.nspin, -1).clone()
+    orb = _Orbitals(system, nb, wdtype, dev)
+    for spin in range(system.nspin):
+        for ik, sphere in enumerate(system.wave_spheres):
+            if wavefunctions is not None:
+                w = wavefunctions[spin][ik]
+                w = w if isinstance(w, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(w))
+                orb.set(spin, ik, w.to(dev, wdtype))
+            else:
+                orb.set(spin, ik, random_bands(len(sphere), nb, sphere.kinetic_energy,
+                                               seed=12345 + 991 * spin + ik, dtype=wdtype))
+    eng.reserve("complex128" if wdtype == torch.complex128 else "complex64", nb)
+    kin_dev = [torch.from_numpy(s.kinetic_energy).to(dev) for s in system.wave_spheres]
+    dij_dev = torch.from_numpy(system.projectors[0].dij).to(dev, torch.complex128) if eng.nproj else None
+    vloc = torch.from_numpy(system.v_local.ravel()).to(dev)
+    mixer = create_mixer(config.scf.mixing, system)
+
+    threshold = config.scf.tol_energy * natoms * EV_IN_HARTREE
+    history, trace, step_times = [], [], []
+    previous = np.inf
+    residual = np.inf
+    converged = False
+    energies = Energies(ewald=system.ewald)
+    occ_result = None
+    eigenvalues = np.zeros((system.nspin, system.nkpoints, nb))
+    rho_out = rho_in
+    iteration = 0
+    for iteration in range(1, config.scf.max_steps + 1):
+        t_step = time.perf_counter()
+        if policy == "mixed" and orb.dtype == torch.complex64 and residual < config.engine.refine_below:
+            orb.to(torch.complex128)
+            eng.reserve("complex128", nb)
+        prec_name = "complex64" if orb.dtype == torch.complex64 else "complex128"
+        trace.append(prec_name)
+        veff, _, _ = effective_potential(system, rho_in)
+        H = Hamiltonian(system, veff, precision=prec_name)
+        tol = float(np.clip(1e-3 * min(residual, 1.0), 1e-11, 1e-6))
+        if orb.dtype == torch.complex64:
+            tol = max(tol, 1e-5)  # below ~1e-5 an FP32 residual is rounding noise
+        maxit = 40 if iteration == 1 else 20
+        eigenvalues = np.empty((system.nspin, system.nkpoints, nb))
+        for spin in range(system.nspin):
+            for ik, sphere in enumerate(system.wave_spheres):
+                res = davidson(lambda b, ik=ik, spin=spin: H.apply(b, ik, spin), orb.block(spin, ik),
+                               kin_dev[ik], tolerance=tol, max_iterations=maxit)
+                eigenvalues[spin, ik] = res.eigenvalues.cpu().numpy()
+                orb.set(spin, ik, res.coefficients)
+        occ_result = compute_occupations(eigenvalues, system.kpoints.weights, system.nelectrons,
+                                         scheme=config.occupations.scheme, smearing=smearing,
+                                         order=config.occupations.order, nspin=system.nspin)
+        occ = occ_result.occupations
+        rho_out = _density_out(system, orb, occ)
+        e_h, _ = ops.hartree(rho_out.sum(0))
+        xc_d = rho_out
+        if system.core_density is not None:
+            xc_d = rho_out + torch.from_numpy(system.core_density.ravel()).to(dev)[None] / system.nspin
+        e_xc, _ = ops.lda(xc_d)
+        energies = Energies(
+            kinetic=_kinetic_energy(system, orb, occ, kin_dev),
+            local=float((vloc * rho_out.sum(0)).sum()) * dv,
+            hartree=float(e_h), xc=float(e_xc),
+            nonlocal_=_nonlocal_energy(system, orb, occ, dij_dev),
+            ewald=system.ewald, entropy=occ_result.entropy_term)
+        band_sum = 2.0 / system.nspin * float(np.einsum("k,skn,skn->", system.kpoints.weights, occ, eigenvalues))
+        local_e = float((veff.reshape(system.nspin, -1) * rho_out).sum()) * dv
+        identity = band_sum - (energies.kinetic + local_e + energies.nonlocal_)
+        residual = float((rho_out - rho_in).abs().sum()) * dv / system.nelectrons
+        energy = energies.free_energy
+        delta = energy - previous
+        history.append((energy, residual, identity))
+        step_times.append(time.perf_counter() - t_step)
+        log(f"  {iteration:4d} {energy * HARTREE_IN_EV:18.9f} {delta * HARTREE_IN_EV / natoms:14.2e} "
+            f"{residual:13.3e} {identity * HARTREE_IN_EV:12.2e} {step_times[-1]:9.2f} {prec_name}")
+        if iteration > 1 and abs(delta) < threshold and residual < config.scf.tol_density:
+            if not (policy == "mixed" and orb.dtype == torch.complex64):
+                converged = True
+                break
+        previous = energy
+        rho_in = mixer(rho_in, rho_out)
+
+    wfs = [[orb.block(spin, ik).clone() for ik in range(system.nkpoints)] for spin in range(system.nspin)]
+    dens = rho_out.reshape(system.nspin, *system.grid.shape).cpu().numpy()
+    return SCFResult(
+        converged=converged, iterations=iteration, energies=energies, eigenvalues=eigenvalues,
+        occupations=occ_result.occupations, fermi_level=occ_result.fermi_level, gap=occ_result.gap,
+        magnetization=occ_result.magnetization, density=dens, wavefunctions=wfs, history=history,
+        electron_count=float(dens.sum()) * dv, seconds=time.perf_counter() - started,
+        precision_trace=trace, seconds_per_iteration=step_times)

@@ -127,6 +127,11 @@ AMA_API int ama_set_grid_filter(AmaEngine* engine, int32_t slot, const double* f
 AMA_API int ama_grid_filter(AmaEngine* engine, int32_t slot, int32_t energy_slot,
                             const double* in, double* out, double* energy, void* stream);
 
+/* Forward transform of a real grid field to natural FFT order (device FP64 in
+ * [n1*n2*n3], device complex128 out [n1*n2*n3]): out[G] = (1/N) sum_r in(r) e^{-iG.r}.
+ * Replaces FFTGrid.to_reciprocal on a density (basis/fft.py:228-235). */
+AMA_API int ama_grid_fft_forward(AmaEngine* engine, const double* in, void* out, void* stream);
+
 /* LDA exchange plus Perdew-Zunger 1981 correlation on a spin-resolved density
  * (device FP64, rho [2][npoints]); writes eps_xc [npoints] and v_xc [2][npoints].
  * Replaces lda.exchange + lda.correlation_pz81 (xc/lda.py:122-142,203-262). */
@@ -136,6 +141,12 @@ AMA_API int ama_lda_pz(const double* rho, int64_t npoints, double* eps, double* 
  * interleaved complex, overwritten by eigenvectors as columns); eigenvalues ascending.
  * Replaces scipy.linalg.eigh in rayleigh_ritz (scf/eigen/subspace.py:74). */
 AMA_API int ama_heev(int32_t n, void* matrices, double* eigenvalues, int32_t batch, void* stream);
+
+/* Inverse Cholesky factor of `batch` Hermitian positive-definite FP64 matrices (device,
+ * row-major, interleaved complex): on return each holds L^{-1} (lower triangular) with
+ * S = L L^H. AMA_ERR_NOT_SPD if a pivot is not positive. Replaces the cholesky +
+ * solve_triangular pair of orthonormalize (scf/eigen/subspace.py:17-32). */
+AMA_API int ama_potrf_inv(int32_t n, void* matrices, int32_t batch, void* stream);
 
 #ifdef __cplusplus
 }

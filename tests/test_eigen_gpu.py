@@ -1,0 +1,88 @@
+"""GPU Davidson and subspace steps against dense eigh, the oracle and the reference."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+
+def _hermitian(n, seed):
+    rng = np.random.default_rng(seed)
+    a = rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n))
+    kinetic = np.linspace(0.0, 20.0, n)
+    return 0.05 * (a + a.conj().T) + np.diag(kinetic), kinetic
+
+
+def test_davidson_matches_dense_eigh():
+    """Mirror of the reference's test_eigen.py:28-41 (numpy callable, numpy guess)."""
+    from amaterasu_b200.eigen import davidson
+    matrix, kinetic = _hermitian(80, 0)
+    rng = np.random.default_rng(1)
+    guess = rng.normal(size=(6, 80)) + 1j * rng.normal(size=(6, 80))
+    res = davidson(lambda b: b @ matrix.T, guess, kinetic, tolerance=1e-10, max_iterations=100)
+    exact = np.linalg.eigvalsh(matrix)[:6]
+    assert res.converged
+    np.testing.assert_allclose(res.eigenvalues, exact, rtol=0, atol=1e-10)
+    c = res.coefficients
+    np.testing.assert_allclose(c @ c.conj().T, np.eye(6), atol=1e-12)
+    # |d eps| <= ||r|| (test_eigen.py:44-55)
+    assert np.all(np.abs(res.eigenvalues - exact) <= res.residual_norms + 1e-12)
+
+
+def test_subspace_pieces_match_reference(mini_system):
+    from amaterasu_b200.eigen import orthonormalize, random_bands, rayleigh_ritz, teter_payne_allan
+    from amaterasu_b200.hamiltonian import Hamiltonian
+    g = golden("mini.npz")
+    s = mini_system
+    H = Hamiltonian(s, g["veff"])
+    for ik, sphere in enumerate(s.wave_spheres):
+        guess = random_bands(len(sphere), s.nbands, sphere.kinetic_energy, seed=12345 + ik)
+        np.testing.assert_allclose(guess, g[f"guess{ik}"], rtol=0, atol=1e-12)
+        basis = orthonormalize(g[f"psi{ik}"][:4])
+        np.testing.assert_allclose(basis, g[f"ortho{ik}"], rtol=0, atol=1e-11)
+        e, x, hx = rayleigh_ritz(basis, H.apply(basis, ik), 3)
+        np.testing.assert_allclose(e, g[f"rr_eig{ik}"], rtol=0, atol=1e-11)
+        # the Ritz vectors themselves: H x is the rotated H basis and x^H H x = diag(e)
+        np.testing.assert_allclose(hx, H.apply(x, ik), rtol=0, atol=1e-11)
+        np.testing.assert_allclose(x.conj() @ hx.T, np.diag(e), rtol=0, atol=1e-11)
+        out = teter_payne_allan(g[f"tpa_in{ik}"], sphere.kinetic_energy, g[f"tpa_ref{ik}"])
+        np.testing.assert_allclose(out, g[f"tpa_out{ik}"], rtol=0, atol=1e-13)
+
+
+@pytest.mark.parametrize("device_block", [False, True])
+def test_davidson_engine_matches_reference(mini_system, device_block):
+    from amaterasu_b200.eigen import davidson
+    from amaterasu_b200.hamiltonian import Hamiltonian
+    g = golden("mini.npz")
+    s = mini_system
+    H = Hamiltonian(s, g["veff"])
+    for ik, sphere in enumerate(s.wave_spheres):
+        guess = g[f"guess{ik}"]
+        if device_block:
+            guess = torch.from_numpy(guess).cuda()
+        res = davidson(lambda b, ik=ik: H.apply(b, ik), guess, sphere.kinetic_energy, tolerance=1e-9,
+                       max_iterations=60)
+        eig = res.eigenvalues.cpu().numpy() if device_block else res.eigenvalues
+        np.testing.assert_allclose(eig, g[f"dav_eig{ik}"], rtol=0, atol=1e-9)
+
+
+def test_davidson_complex64_working_precision(mini_system):
+    from amaterasu_b200.eigen import davidson
+    from amaterasu_b200.hamiltonian import Hamiltonian
+    g = golden("mini.npz")
+    s = mini_system
+    H = Hamiltonian(s, g["veff"], precision="complex64")
+    guess = torch.from_numpy(g["guess0"]).cuda().to(torch.complex64)
+    res = davidson(lambda b: H.apply(b, 0), guess, s.wave_spheres[0].kinetic_energy, tolerance=1e-4,
+                   max_iterations=60)
+    np.testing.assert_allclose(res.eigenvalues.cpu().numpy()[:5], g["dav_eig0"][:5], rtol=0, atol=2e-5)
+
+
+def test_solve_dispatch_errors():
+    from amaterasu_b200.eigen import solve
+    with pytest.raises(NotImplementedError):
+        solve("lobpcg", lambda b: b, np.eye(2), np.zeros(2))
+    with pytest.raises(NotImplementedError):
+        solve("davidson", lambda b: b, np.eye(2), np.zeros(2), apply_overlap=lambda b: b)
