@@ -21,6 +21,9 @@
 
 namespace ama {
 
+// Every FFT-stage kernel runs with this many threads per CTA; the passes stride by it.
+constexpr int kFftThreads = 256;
+
 // ---------------------------------------------------------------- codelets
 // In-register DFT of length R with sign S (+1 backward, -1 forward), natural order in
 // and out. Odd lengths use the symmetric pair form; even lengths split radix-2.
@@ -124,32 +127,46 @@ __device__ __forceinline__ void dft_reg(C (&v)[R]) {
 template <int RA, int S, bool TW, typename C>
 __device__ __forceinline__ void strided_task(C* __restrict__ base, int es, int n, int b,
                                              const C* __restrict__ tw) {
+  if constexpr (RA > 1) {
   const int B = n / RA;
   C v[RA];
 #pragma unroll
   for (int a = 0; a < RA; ++a) v[a] = base[(a * B + b) * es];
   dft_reg<RA, S>(v);
   if constexpr (TW) {
+    int idx = 0;  // (b * c) mod n, advanced without a division (b < n)
 #pragma unroll
-    for (int c = 1; c < RA; ++c) v[c] = cmul(v[c], tw[(b * c) % n]);
+    for (int c = 1; c < RA; ++c) {
+      idx += b;
+      if (idx >= n) idx -= n;
+      v[c] = cmul(v[c], tw[idx]);
+    }
   }
 #pragma unroll
   for (int c = 0; c < RA; ++c) base[(c * B + b) * es] = v[c];
+  }
 }
 
 template <int RB, int S, bool TW, typename C>
 __device__ __forceinline__ void contig_task(C* __restrict__ base, int es, int n, int c,
                                             const C* __restrict__ tw) {
+  if constexpr (RB > 1) {
   C v[RB];
 #pragma unroll
   for (int d = 0; d < RB; ++d) v[d] = base[(c * RB + d) * es];
   dft_reg<RB, S>(v);
   if constexpr (TW) {
+    int idx = 0;  // (c * e) mod n
 #pragma unroll
-    for (int e = 1; e < RB; ++e) v[e] = cmul(v[e], tw[(c * e) % n]);
+    for (int e = 1; e < RB; ++e) {
+      idx += c;
+      if (idx >= n) idx -= n;
+      v[e] = cmul(v[e], tw[idx]);
+    }
   }
 #pragma unroll
   for (int d = 0; d < RB; ++d) base[(c * RB + d) * es] = v[d];
+  }
 }
 
 // Column mode: consecutive threads take consecutive columns (conflict-free smem).
@@ -157,7 +174,7 @@ template <int RA, int S, bool TW, typename C>
 __device__ void strided_cols(C* sm, int n, int ncols, const C* tw) {
   const int B = n / RA;
   const int tasks = B * ncols;
-  for (int t = threadIdx.x; t < tasks; t += blockDim.x) {
+  for (int t = threadIdx.x; t < tasks; t += kFftThreads) {
     const int col = t % ncols, b = t / ncols;
     strided_task<RA, S, TW>(sm + col, ncols, n, b, tw);
   }
@@ -166,7 +183,7 @@ template <int RB, int S, bool TW, typename C>
 __device__ void contig_cols(C* sm, int n, int ncols, const C* tw) {
   const int A = n / RB;
   const int tasks = A * ncols;
-  for (int t = threadIdx.x; t < tasks; t += blockDim.x) {
+  for (int t = threadIdx.x; t < tasks; t += kFftThreads) {
     const int col = t % ncols, c = t / ncols;
     contig_task<RB, S, TW>(sm + col, ncols, n, c, tw);
   }
@@ -176,7 +193,7 @@ template <int RA, int S, bool TW, typename C>
 __device__ void strided_rows(C* sm, int n, int ld, const int* rows, int nrows, const C* tw) {
   const int B = n / RA;
   const int tasks = B * nrows;
-  for (int t = threadIdx.x; t < tasks; t += blockDim.x) {
+  for (int t = threadIdx.x; t < tasks; t += kFftThreads) {
     const int b = t % B, r = rows[t / B];
     strided_task<RA, S, TW>(sm + r * ld, 1, n, b, tw);
   }
@@ -185,7 +202,7 @@ template <int RB, int S, bool TW, typename C>
 __device__ void contig_rows(C* sm, int n, int ld, const int* rows, int nrows, const C* tw) {
   const int A = n / RB;
   const int tasks = A * nrows;
-  for (int t = threadIdx.x; t < tasks; t += blockDim.x) {
+  for (int t = threadIdx.x; t < tasks; t += kFftThreads) {
     const int c = t % A, r = rows[t / A];
     contig_task<RB, S, TW>(sm + r * ld, 1, n, c, tw);
   }

@@ -21,6 +21,7 @@
 #include "common.cuh"
 #include "dft.cuh"
 #include "gemm.cuh"
+#include "engine_impl.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -29,8 +30,6 @@
 #include <vector>
 
 namespace ama {
-
-struct AxisPlan { int n, A, B; };
 
 static bool split_length(int n, AxisPlan* out) {
   // n = A*B with A, B in the codelet set; minimise max(A, B), prefer A >= B.
@@ -48,49 +47,7 @@ static bool split_length(int n, AxisPlan* out) {
 }
 
 
-struct DeviceTables {
-  int* plane_x = nullptr;      // [nslots]
-  int* slot_of_x = nullptr;    // [n1] -> slot or -1
-  int2* entries = nullptr;     // [sum npw]: (g, y*n3+z) grouped by (k, slot)
-  int* entry_start = nullptr;  // [nk*(nslots+1)]
-  int* rows = nullptr;         // concatenated y rows per (k, slot)
-  int* row_start = nullptr;    // [nk*(nslots+1)]
-  int64_t* pw_off = nullptr;   // [nk+1]
-  int* npw = nullptr;          // [nk]
-  double* kin64 = nullptr;     // [sum npw]
-  float* kin32 = nullptr;
-  void* tw[2][3][2] = {};      // [prec][axis][0 backward,1 forward]
-  void* proj[2] = {};          // [prec] B, k-major (nproj, npw_k) blocks
-  void* dproj[2] = {};         // [prec] D.B
-  double* v64 = nullptr;       // [nspin][N] permuted, /N
-  float* v32 = nullptr;
-};
-
 }  // namespace ama
-
-using namespace ama;
-
-struct AmaEngine {
-  AxisPlan ax[3];
-  int64_t N = 0;
-  int nk = 0, nspin = 1, nproj = 0, nslots = 0;
-  uint32_t precisions = 0;
-  std::vector<int> npw;
-  std::vector<int64_t> pw_off;
-  int max_npw = 0;
-  int max_rows = 0;
-  DeviceTables d;
-  bool has_potential = false;
-  // workspaces (grown on demand)
-  void* work[2] = {};
-  size_t work_bytes[2] = {};
-  void* ws_proj[2] = {};       // P = psi B^H
-  size_t ws_proj_bytes[2] = {};
-  void* ws_part[2] = {};       // split-K partials
-  size_t ws_part_bytes[2] = {};
-  double* ws_dens = nullptr;   // permuted density accumulator
-  size_t ws_dens_bytes = 0;
-};
 
 namespace {
 
@@ -132,117 +89,157 @@ __device__ __forceinline__ void load_twiddles(C* dst, const C* src, int n) {
   for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
 }
 
-template <typename T>
-__global__ void stage_a_kernel(HpsiView v, const cx_t<T>* __restrict__ tw_y,
-                               const cx_t<T>* __restrict__ tw_z,
-                               const cx_t<T>* __restrict__ psi, cx_t<T>* __restrict__ work) {
+// Grid sizes: compile-time for the engine's common grids (all index arithmetic folds to
+// constants), read from the view otherwise.
+struct DynDims {
+  template <class V> __device__ static __forceinline__ int n1(const V& v) { return v.n1; }
+  template <class V> __device__ static __forceinline__ int a1(const V& v) { return v.A1; }
+  template <class V> __device__ static __forceinline__ int n2(const V& v) { return v.n2; }
+  template <class V> __device__ static __forceinline__ int a2(const V& v) { return v.A2; }
+  template <class V> __device__ static __forceinline__ int n3(const V& v) { return v.n3; }
+  template <class V> __device__ static __forceinline__ int a3(const V& v) { return v.A3; }
+};
+template <int N1, int A1, int N2, int A2, int N3, int A3> struct FixDims {
+  template <class V> __device__ static constexpr int n1(const V&) { return N1; }
+  template <class V> __device__ static constexpr int a1(const V&) { return A1; }
+  template <class V> __device__ static constexpr int n2(const V&) { return N2; }
+  template <class V> __device__ static constexpr int a2(const V&) { return A2; }
+  template <class V> __device__ static constexpr int n3(const V&) { return N3; }
+  template <class V> __device__ static constexpr int a3(const V&) { return A3; }
+};
+
+#define AMA_DIMS(D, v)                                                    \
+  const int n1 = D::n1(v), A1 = D::a1(v), B1 = n1 / A1;                   \
+  const int n2 = D::n2(v), A2 = D::a2(v), B2 = n2 / A2;                   \
+  const int n3 = D::n3(v), A3 = D::a3(v), B3 = n3 / A3;                   \
+  const int plane = n2 * n3;                                              \
+  (void)B1; (void)B2; (void)B3; (void)A1; (void)A2; (void)A3; (void)plane;
+
+template <typename C>
+__device__ __forceinline__ void load_tw(C* dst, const C* src, int n) {
+  for (int i = threadIdx.x; i < n; i += kFftThreads) dst[i] = src[i];
+}
+
+template <typename T, class D>
+__global__ void __launch_bounds__(kFftThreads)
+stage_a_kernel(HpsiView v, const cx_t<T>* __restrict__ tw_y, const cx_t<T>* __restrict__ tw_z,
+               const cx_t<T>* __restrict__ psi, cx_t<T>* __restrict__ work) {
   using C = cx_t<T>;
+  AMA_DIMS(D, v)
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* plane = reinterpret_cast<C*>(smem_raw);
-  C* sty = plane + v.plane_elems;
-  C* stz = sty + v.n2;
-  int* rows = reinterpret_cast<int*>(stz + v.n3);
+  C* pl = reinterpret_cast<C*>(smem_raw);
+  C* sty = pl + plane;
+  C* stz = sty + n2;
+  int* rows = reinterpret_cast<int*>(stz + n3);
 
   const int slot = blockIdx.x;
   const int gb = blockIdx.y;
-  const int kl = gb / v.nbands, band = gb % v.nbands;
+  const int kl = gb / v.nbands, band = gb - kl * v.nbands;
   const int k = v.k_first + kl;
   const int npw = v.npw[k];
   const C* src = psi + (v.pw_off[k] - v.pw_off[v.k_first]) * v.nbands + (int64_t)band * npw;
 
-  load_twiddles(sty, tw_y, v.n2);
-  load_twiddles(stz, tw_z, v.n3);
-  for (int64_t i = threadIdx.x; i < v.plane_elems; i += blockDim.x) plane[i] = mk<C>(0, 0);
+  load_tw(sty, tw_y, n2);
+  load_tw(stz, tw_z, n3);
+  for (int i = threadIdx.x; i < plane; i += kFftThreads) pl[i] = mk<C>(0, 0);
   const int rs = v.row_start[k * (v.nslots + 1) + slot];
   const int nrows = v.row_start[k * (v.nslots + 1) + slot + 1] - rs;
-  for (int i = threadIdx.x; i < nrows; i += blockDim.x) rows[i] = v.rows[rs + i];
+  for (int i = threadIdx.x; i < nrows; i += kFftThreads) rows[i] = v.rows[rs + i];
   __syncthreads();
   const int es = v.entry_start[k * (v.nslots + 1) + slot];
   const int ee = v.entry_start[k * (v.nslots + 1) + slot + 1];
-  for (int t = es + threadIdx.x; t < ee; t += blockDim.x) {
+  for (int t = es + threadIdx.x; t < ee; t += kFftThreads) {
     const int2 en = v.entries[t];
-    plane[en.y] = src[en.x];
+    pl[en.y] = src[en.x];
   }
   __syncthreads();
-  dft_rows<+1>(plane, v.n3, v.A3, v.B3, v.n3, rows, nrows, stz);
-  dft_cols<+1>(plane, v.n2, v.A2, v.B2, v.n3, sty);
-  C* dst = work + (int64_t)gb * v.band_elems + (int64_t)slot * v.plane_elems;
-  for (int64_t i = threadIdx.x; i < v.plane_elems; i += blockDim.x) dst[i] = plane[i];
+  dft_rows<+1>(pl, n3, A3, B3, n3, rows, nrows, stz);
+  dft_cols<+1>(pl, n2, A2, B2, n3, sty);
+  C* dst = work + (int64_t)gb * v.band_elems + (int64_t)slot * plane;
+  for (int i = threadIdx.x; i < plane; i += kFftThreads) dst[i] = pl[i];
 }
 
-template <typename T>
-__global__ void stage_b_kernel(HpsiView v, const cx_t<T>* __restrict__ tw_xb,
-                               const cx_t<T>* __restrict__ tw_xf, const T* __restrict__ vpot,
-                               cx_t<T>* __restrict__ work) {
+// Load the slot rows at one y into an (n1, n3) slab, zero elsewhere, backward x transform.
+template <typename T, class D>
+__device__ __forceinline__ void slab_load_backward(const HpsiView& v, const cx_t<T>* wb, cx_t<T>* slab,
+                                                   const cx_t<T>* twb) {
   using C = cx_t<T>;
+  AMA_DIMS(D, v)
+  for (int e = threadIdx.x; e < n1 * n3; e += kFftThreads) {
+    const int x = e / n3, z = e - x * n3;
+    const int slot = v.slot_of_x[x];
+    slab[e] = slot >= 0 ? wb[(int64_t)slot * plane + z] : mk<C>(0, 0);
+  }
+  __syncthreads();
+  dft_cols<+1>(slab, n1, A1, B1, n3, twb);
+}
+
+template <typename T, class D>
+__global__ void __launch_bounds__(kFftThreads)
+stage_b_kernel(HpsiView v, const cx_t<T>* __restrict__ tw_xb, const cx_t<T>* __restrict__ tw_xf,
+               const T* __restrict__ vpot, cx_t<T>* __restrict__ work) {
+  using C = cx_t<T>;
+  AMA_DIMS(D, v)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* slab = reinterpret_cast<C*>(smem_raw);  // [n1][n3]
-  C* twb = slab + (int64_t)v.n1 * v.n3;
-  C* twf = twb + v.n1;
+  C* twb = slab + n1 * n3;
+  C* twf = twb + n1;
   const int y = blockIdx.x;
   const int gb = blockIdx.y;
-  load_twiddles(twb, tw_xb, v.n1);
-  load_twiddles(twf, tw_xf, v.n1);
-  C* wb = work + (int64_t)gb * v.band_elems + (int64_t)y * v.n3;
-  const int total = v.n1 * v.n3;
-  for (int e = threadIdx.x; e < total; e += blockDim.x) {
-    const int x = e / v.n3, z = e % v.n3;
-    const int slot = v.slot_of_x[x];
-    slab[e] = slot >= 0 ? wb[(int64_t)slot * v.plane_elems + z] : mk<C>(0, 0);
+  load_tw(twb, tw_xb, n1);
+  load_tw(twf, tw_xf, n1);
+  C* wb = work + (int64_t)gb * v.band_elems + (int64_t)y * n3;
+  slab_load_backward<T, D>(v, wb, slab, twb);
+  const T* vy = vpot + (int64_t)y * n3;
+  for (int e = threadIdx.x; e < n1 * n3; e += kFftThreads) {
+    const int x = e / n3, z = e - x * n3;
+    slab[e] = cscale(slab[e], vy[(int64_t)x * plane + z]);
   }
   __syncthreads();
-  dft_cols<+1>(slab, v.n1, v.A1, v.B1, v.n3, twb);
-  const T* vy = vpot + (int64_t)y * v.n3;
-  const int64_t xstride = (int64_t)v.n2 * v.n3;
-  for (int e = threadIdx.x; e < total; e += blockDim.x) {
-    const int x = e / v.n3, z = e % v.n3;
-    slab[e] = cscale(slab[e], vy[x * xstride + z]);
-  }
-  __syncthreads();
-  dft_cols<-1>(slab, v.n1, v.A1, v.B1, v.n3, twf);
-  const int ts = v.nslots * v.n3;
-  for (int e = threadIdx.x; e < ts; e += blockDim.x) {
-    const int slot = e / v.n3, z = e % v.n3;
-    wb[(int64_t)slot * v.plane_elems + z] = slab[v.plane_x[slot] * v.n3 + z];
+  dft_cols<-1>(slab, n1, A1, B1, n3, twf);
+  for (int e = threadIdx.x; e < v.nslots * n3; e += kFftThreads) {
+    const int slot = e / n3, z = e - slot * n3;
+    wb[(int64_t)slot * plane + z] = slab[v.plane_x[slot] * n3 + z];
   }
 }
 
-template <typename T>
-__global__ void stage_c_kernel(HpsiView v, const cx_t<T>* __restrict__ tw_y,
-                               const cx_t<T>* __restrict__ tw_z, const T* __restrict__ kin,
-                               const cx_t<T>* __restrict__ psi, const cx_t<T>* __restrict__ work,
-                               cx_t<T>* __restrict__ hpsi) {
+template <typename T, class D>
+__global__ void __launch_bounds__(kFftThreads)
+stage_c_kernel(HpsiView v, const cx_t<T>* __restrict__ tw_y, const cx_t<T>* __restrict__ tw_z,
+               const T* __restrict__ kin, const cx_t<T>* __restrict__ psi,
+               const cx_t<T>* __restrict__ work, cx_t<T>* __restrict__ hpsi) {
   using C = cx_t<T>;
+  AMA_DIMS(D, v)
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* plane = reinterpret_cast<C*>(smem_raw);
-  C* sty = plane + v.plane_elems;
-  C* stz = sty + v.n2;
-  int* rows = reinterpret_cast<int*>(stz + v.n3);
+  C* pl = reinterpret_cast<C*>(smem_raw);
+  C* sty = pl + plane;
+  C* stz = sty + n2;
+  int* rows = reinterpret_cast<int*>(stz + n3);
 
   const int slot = blockIdx.x;
   const int gb = blockIdx.y;
-  const int kl = gb / v.nbands, band = gb % v.nbands;
+  const int kl = gb / v.nbands, band = gb - kl * v.nbands;
   const int k = v.k_first + kl;
   const int npw = v.npw[k];
   const int64_t boff = (v.pw_off[k] - v.pw_off[v.k_first]) * v.nbands + (int64_t)band * npw;
 
-  load_twiddles(sty, tw_y, v.n2);
-  load_twiddles(stz, tw_z, v.n3);
-  const C* srcw = work + (int64_t)gb * v.band_elems + (int64_t)slot * v.plane_elems;
-  for (int64_t i = threadIdx.x; i < v.plane_elems; i += blockDim.x) plane[i] = srcw[i];
+  load_tw(sty, tw_y, n2);
+  load_tw(stz, tw_z, n3);
+  const C* srcw = work + (int64_t)gb * v.band_elems + (int64_t)slot * plane;
+  for (int i = threadIdx.x; i < plane; i += kFftThreads) pl[i] = srcw[i];
   const int rs = v.row_start[k * (v.nslots + 1) + slot];
   const int nrows = v.row_start[k * (v.nslots + 1) + slot + 1] - rs;
-  for (int i = threadIdx.x; i < nrows; i += blockDim.x) rows[i] = v.rows[rs + i];
+  for (int i = threadIdx.x; i < nrows; i += kFftThreads) rows[i] = v.rows[rs + i];
   __syncthreads();
-  dft_cols<-1>(plane, v.n2, v.A2, v.B2, v.n3, sty);
-  dft_rows<-1>(plane, v.n3, v.A3, v.B3, v.n3, rows, nrows, stz);
+  dft_cols<-1>(pl, n2, A2, B2, n3, sty);
+  dft_rows<-1>(pl, n3, A3, B3, n3, rows, nrows, stz);
   const int es = v.entry_start[k * (v.nslots + 1) + slot];
   const int ee = v.entry_start[k * (v.nslots + 1) + slot + 1];
   const T* kk = kin + v.pw_off[k];
-  for (int t = es + threadIdx.x; t < ee; t += blockDim.x) {
+  for (int t = es + threadIdx.x; t < ee; t += kFftThreads) {
     const int2 en = v.entries[t];
     const C p = psi[boff + en.x];
-    C r = plane[en.y];
+    C r = pl[en.y];
     const T tg = kk[en.x];
     r.x += tg * p.x;
     r.y += tg * p.y;
@@ -250,38 +247,69 @@ __global__ void stage_c_kernel(HpsiView v, const cx_t<T>* __restrict__ tw_y,
   }
 }
 
-// density: backward transform as stage A, x backward as in stage B, then |u|^2 weighted
-// accumulation into a permuted FP64 grid (one CTA per (y, band) slab, atomics per point).
-template <typename T>
-__global__ void density_b_kernel(HpsiView v, const cx_t<T>* __restrict__ tw_xb,
-                                 const cx_t<T>* __restrict__ work, const double* __restrict__ w,
-                                 double* __restrict__ acc) {
+// density: stage A output -> backward x, then weighted |u|^2 into a permuted FP64 grid.
+template <typename T, class D>
+__global__ void __launch_bounds__(kFftThreads)
+density_b_kernel(HpsiView v, const cx_t<T>* __restrict__ tw_xb, const cx_t<T>* __restrict__ work,
+                 const double* __restrict__ w, double* __restrict__ acc) {
   using C = cx_t<T>;
+  AMA_DIMS(D, v)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* slab = reinterpret_cast<C*>(smem_raw);
-  C* twb = slab + (int64_t)v.n1 * v.n3;
+  C* twb = slab + n1 * n3;
   const int y = blockIdx.x;
   const int gb = blockIdx.y;
   const double weight = w[gb];
   if (weight == 0.0) return;
-  load_twiddles(twb, tw_xb, v.n1);
-  const C* wb = work + (int64_t)gb * v.band_elems + (int64_t)y * v.n3;
-  const int total = v.n1 * v.n3;
-  for (int e = threadIdx.x; e < total; e += blockDim.x) {
-    const int x = e / v.n3, z = e % v.n3;
-    const int slot = v.slot_of_x[x];
-    slab[e] = slot >= 0 ? wb[(int64_t)slot * v.plane_elems + z] : mk<C>(0, 0);
-  }
-  __syncthreads();
-  dft_cols<+1>(slab, v.n1, v.A1, v.B1, v.n3, twb);
-  const int64_t xstride = (int64_t)v.n2 * v.n3;
-  for (int e = threadIdx.x; e < total; e += blockDim.x) {
-    const int x = e / v.n3, z = e % v.n3;
+  load_tw(twb, tw_xb, n1);
+  const C* wb = work + (int64_t)gb * v.band_elems + (int64_t)y * n3;
+  slab_load_backward<T, D>(v, wb, slab, twb);
+  for (int e = threadIdx.x; e < n1 * n3; e += kFftThreads) {
+    const int x = e / n3, z = e - x * n3;
     const C u = slab[e];
-    const double m2 = (double)u.x * (double)u.x + (double)u.y * (double)u.y;
-    atomicAdd(acc + x * xstride + (int64_t)y * v.n3 + z, weight * m2);
+    atomicAdd(acc + (int64_t)x * plane + (int64_t)y * n3 + z,
+              weight * ((double)u.x * (double)u.x + (double)u.y * (double)u.y));
   }
 }
+
+template <typename T, class D>
+void fill_stage_table(const void** fn) {
+  fn[0] = (const void*)stage_a_kernel<T, D>;
+  fn[1] = (const void*)stage_b_kernel<T, D>;
+  fn[2] = (const void*)stage_c_kernel<T, D>;
+  fn[3] = (const void*)density_b_kernel<T, D>;
+}
+
+// Grids with compile-time kernels (cubic cells of the benchmark workloads); any other grid
+// runs the same kernels with sizes read at run time.
+template <typename T>
+void select_stage_table(const AxisPlan* ax, const void** fn) {
+#define AMA_FIX(N1, A1, N2, A2, N3, A3)                                                         \
+  if (ax[0].n == N1 && ax[0].A == A1 && ax[1].n == N2 && ax[1].A == A2 && ax[2].n == N3 &&      \
+      ax[2].A == A3) {                                                                           \
+    fill_stage_table<T, FixDims<N1, A1, N2, A2, N3, A3>>(fn);                                   \
+    return;                                                                                      \
+  }
+  AMA_FIX(20, 5, 20, 5, 20, 5)
+  AMA_FIX(25, 5, 25, 5, 25, 5)
+  AMA_FIX(35, 7, 35, 7, 35, 7)
+  AMA_FIX(36, 6, 36, 6, 36, 6)
+  AMA_FIX(42, 7, 42, 7, 42, 7)
+  AMA_FIX(84, 12, 84, 12, 84, 12)
+  AMA_FIX(108, 12, 108, 12, 108, 12)
+#undef AMA_FIX
+  fill_stage_table<T, DynDims>(fn);
+}
+
+template <typename T>
+using StageAFn = void (*)(HpsiView, const cx_t<T>*, const cx_t<T>*, const cx_t<T>*, cx_t<T>*);
+template <typename T>
+using StageBFn = void (*)(HpsiView, const cx_t<T>*, const cx_t<T>*, const T*, cx_t<T>*);
+template <typename T>
+using StageCFn = void (*)(HpsiView, const cx_t<T>*, const cx_t<T>*, const T*, const cx_t<T>*,
+                          const cx_t<T>*, cx_t<T>*);
+template <typename T>
+using DensFn = void (*)(HpsiView, const cx_t<T>*, const cx_t<T>*, const double*, double*);
 
 template <typename T>
 __global__ void permute_potential_kernel(const double* __restrict__ v, T* __restrict__ out,
@@ -355,7 +383,6 @@ HpsiView make_view(const AmaEngine* e, int k_first, int nbands) {
   return v;
 }
 
-constexpr int kStageThreads = 256;
 
 template <typename T>
 size_t plane_smem(const AmaEngine* e) {
@@ -375,10 +402,13 @@ int set_smem_limits(const AmaEngine* e) {
   AMA_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
   AMA_REQUIRE(ps <= (size_t)optin && ss <= (size_t)optin, AMA_ERR_UNSUPPORTED,
               "grid plane does not fit in shared memory at this precision");
-  AMA_CUDA_TRY(cudaFuncSetAttribute(stage_a_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
-  AMA_CUDA_TRY(cudaFuncSetAttribute(stage_c_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
-  AMA_CUDA_TRY(cudaFuncSetAttribute(stage_b_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
-  AMA_CUDA_TRY(cudaFuncSetAttribute(density_b_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
+  const int p = std::is_same<T, float>::value ? AMA_C64 : AMA_C128;
+  const void** fn = const_cast<AmaEngine*>(e)->stage_fn[p];
+  select_stage_table<T>(e->ax, fn);
+  AMA_CUDA_TRY(cudaFuncSetAttribute(fn[0], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
+  AMA_CUDA_TRY(cudaFuncSetAttribute(fn[2], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
+  AMA_CUDA_TRY(cudaFuncSetAttribute(fn[1], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
+  AMA_CUDA_TRY(cudaFuncSetAttribute(fn[3], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
   return AMA_OK;
 }
 
@@ -401,7 +431,7 @@ int run_fft_stages_a(AmaEngine* e, const HpsiView& v, int nb_total, const void* 
   using C = cx_t<T>;
   const int p = std::is_same<T, float>::value ? AMA_C64 : AMA_C128;
   dim3 ga(e->nslots, nb_total);
-  stage_a_kernel<T><<<ga, kStageThreads, plane_smem<T>(e), s>>>(
+  ((StageAFn<T>)e->stage_fn[p][0])<<<ga, kFftThreads, plane_smem<T>(e), s>>>(
       v, (const C*)e->d.tw[p][1][0], (const C*)e->d.tw[p][2][0], (const C*)psi, (C*)e->work[p]);
   AMA_CHECK_LAUNCH();
   return AMA_OK;
@@ -423,16 +453,19 @@ int hpsi_impl(AmaEngine* e, int k_first, int k_count, int nbands, int spin, cons
   rc = run_fft_stages_a<T>(e, v, (int)nb_total, psi, s);
   if (rc) return rc;
   dim3 gb(e->ax[1].n, nb_total);
-  stage_b_kernel<T><<<gb, kStageThreads, slab_smem<T>(e), s>>>(
+  ((StageBFn<T>)e->stage_fn[p][1])<<<gb, kFftThreads, slab_smem<T>(e), s>>>(
       v, (const C*)e->d.tw[p][0][0], (const C*)e->d.tw[p][0][1], vpot, (C*)e->work[p]);
   AMA_CHECK_LAUNCH();
   dim3 gc(e->nslots, nb_total);
-  stage_c_kernel<T><<<gc, kStageThreads, plane_smem<T>(e), s>>>(
+  ((StageCFn<T>)e->stage_fn[p][2])<<<gc, kFftThreads, plane_smem<T>(e), s>>>(
       v, (const C*)e->d.tw[p][1][1], (const C*)e->d.tw[p][2][1], kin, (const C*)psi,
       (const C*)e->work[p], (C*)hpsi);
   AMA_CHECK_LAUNCH();
 
-  if (e->nproj > 0) {
+  if (e->nproj > 0 && std::is_same<T, float>::value && e->use_tc && e->tc.ready) {
+    rc = nl_tc_run(e, k_first, k_count, nbands, (const float2*)psi, (float2*)hpsi, s);
+    if (rc) return rc;
+  } else if (e->nproj > 0) {
     const size_t el = sizeof(C);
     const size_t pbytes = (size_t)nb_total * e->nproj * el;
     AMA_CUDA_TRY(grow<char>(&e->ws_proj[p], &e->ws_proj_bytes[p], pbytes));
@@ -472,7 +505,7 @@ int density_impl(AmaEngine* e, int k_first, int k_count, int nbands, const void*
   rc = run_fft_stages_a<T>(e, v, (int)nb_total, psi, s);
   if (rc) return rc;
   dim3 gb(e->ax[1].n, nb_total);
-  density_b_kernel<T><<<gb, kStageThreads, slab_smem<T>(e), s>>>(v, (const C*)e->d.tw[p][0][0],
+  ((DensFn<T>)e->stage_fn[p][3])<<<gb, kFftThreads, slab_smem<T>(e), s>>>(v, (const C*)e->d.tw[p][0][0],
                                                                   (const C*)e->work[p], weights, e->ws_dens);
   AMA_CHECK_LAUNCH();
   unpermute_add_kernel<<<592, 256, 0, s>>>(e->ws_dens, rho, e->ax[0].n, e->ax[1].n, e->ax[2].n,
@@ -507,6 +540,7 @@ void free_grid_filters(const AmaEngine* e);
 
 void free_engine(AmaEngine* e) {
   free_grid_filters(e);
+  nl_tc_free(e);
   auto f = [](void* p) { if (p) cudaFree(p); };
   f(e->d.plane_x); f(e->d.slot_of_x); f(e->d.entries); f(e->d.entry_start); f(e->d.rows);
   f(e->d.row_start); f(e->d.pw_off); f(e->d.npw); f(e->d.kin64); f(e->d.kin32); f(e->d.v64); f(e->d.v32);
@@ -668,6 +702,10 @@ extern "C" int ama_engine_create(const AmaSystemDesc* desc, AmaEngine** out) {
         e->d.proj[p] = b; e->d.dproj[p] = d;
       }
     }
+    if (rc) { free_engine(e); return rc; }
+  }
+  if (e->nproj > 0 && (e->precisions & (1u << AMA_C64))) {
+    rc = nl_tc_setup(e);
     if (rc) { free_engine(e); return rc; }
   }
   *out = e;
@@ -977,12 +1015,12 @@ extern "C" int ama_grid_filter(AmaEngine* e, int32_t slot, int32_t energy_slot, 
   AMA_CUDA_TRY(cudaFuncSetAttribute(grid_g2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
   auto T = [&](int axis, int dir) { return (const double2*)e->d.tw[AMA_C128][axis][dir]; };
   const double invN = 1.0 / (double)e->N;
-  grid_g1_kernel<<<g.n1, kStageThreads, ps, s>>>(g, T(1, 1), T(2, 1), in, g_grid_work);
+  grid_g1_kernel<<<g.n1, kFftThreads, ps, s>>>(g, T(1, 1), T(2, 1), in, g_grid_work);
   AMA_CHECK_LAUNCH();
-  grid_g2_kernel<<<g.n2, kStageThreads, ss, s>>>(g, T(0, 1), T(0, 0), it->second.filt[slot], ef, invN,
+  grid_g2_kernel<<<g.n2, kFftThreads, ss, s>>>(g, T(0, 1), T(0, 0), it->second.filt[slot], ef, invN,
                                                   invN * invN, g_grid_work, energy);
   AMA_CHECK_LAUNCH();
-  grid_g3_kernel<<<g.n1, kStageThreads, ps, s>>>(g, T(1, 0), T(2, 0), g_grid_work, out);
+  grid_g3_kernel<<<g.n1, kFftThreads, ps, s>>>(g, T(1, 0), T(2, 0), g_grid_work, out);
   AMA_CHECK_LAUNCH();
   return AMA_OK;
 }
@@ -1003,9 +1041,21 @@ extern "C" int ama_grid_fft_forward(AmaEngine* e, const double* in, void* out, v
   AMA_CUDA_TRY(cudaFuncSetAttribute(grid_g1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
   AMA_CUDA_TRY(cudaFuncSetAttribute(grid_g2f_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
   auto T = [&](int axis, int dir) { return (const double2*)e->d.tw[AMA_C128][axis][dir]; };
-  grid_g1_kernel<<<g.n1, kStageThreads, ps, s>>>(g, T(1, 1), T(2, 1), in, g_grid_work);
+  grid_g1_kernel<<<g.n1, kFftThreads, ps, s>>>(g, T(1, 1), T(2, 1), in, g_grid_work);
   AMA_CHECK_LAUNCH();
-  grid_g2f_kernel<<<g.n2, kStageThreads, ss, s>>>(g, T(0, 1), g_grid_work, (double2*)out, 1.0 / (double)e->N);
+  grid_g2f_kernel<<<g.n2, kFftThreads, ss, s>>>(g, T(0, 1), g_grid_work, (double2*)out, 1.0 / (double)e->N);
   AMA_CHECK_LAUNCH();
   return AMA_OK;
+}
+
+extern "C" int ama_engine_option(AmaEngine* e, int32_t option, int32_t value) {
+  AMA_REQUIRE(e, AMA_ERR_ARG, "null engine");
+  switch (option) {
+    case 0:  // nonlocal products of the complex64 path on the tensor cores (1) or SIMT (0)
+      e->use_tc = value != 0;
+      return AMA_OK;
+    default:
+      ama::set_error("unknown engine option");
+      return AMA_ERR_ARG;
+  }
 }

@@ -1,0 +1,86 @@
+// Internal layout of the engine object shared by the engine's translation units.
+#pragma once
+#include "common.cuh"
+
+#include <cuda.h>
+
+#include <vector>
+
+namespace ama {
+
+struct AxisPlan { int n, A, B; };
+
+struct DeviceTables {
+  int* plane_x = nullptr;      // [nslots]
+  int* slot_of_x = nullptr;    // [n1] -> slot or -1
+  int2* entries = nullptr;     // [sum npw]: (g, y*n3+z) grouped by (k, slot)
+  int* entry_start = nullptr;  // [nk*(nslots+1)]
+  int* rows = nullptr;         // concatenated y rows per (k, slot)
+  int* row_start = nullptr;    // [nk*(nslots+1)]
+  int64_t* pw_off = nullptr;   // [nk+1]
+  int* npw = nullptr;          // [nk]
+  double* kin64 = nullptr;     // [sum npw]
+  float* kin32 = nullptr;
+  void* tw[2][3][2] = {};      // [prec][axis][0 backward,1 forward]
+  void* proj[2] = {};          // [prec] B, k-major (nproj, npw_k) blocks
+  void* dproj[2] = {};         // [prec] D.B
+  double* v64 = nullptr;       // [nspin][N] permuted, /N
+  float* v32 = nullptr;
+};
+
+// Tensor-core (split-TF32) nonlocal path of the complex64 engine.
+struct NlTcState {
+  bool ready = false;
+  int kp = 0;        // padded K of the projection (2*max npw, multiple of 32)
+  int p2 = 0;        // padded rows of the real-expanded projectors (2*nproj, multiple of 128)
+  int k2 = 0;        // padded K of the application (2*nproj, multiple of 32)
+  int mp = 0;        // padded rows of the application (2*max npw, multiple of 128)
+  float* bx[2] = {};   // hi/lo [nk][p2][kp]
+  float* dxt[2] = {};  // hi/lo [nk][mp][k2]
+  CUtensorMap map_bx[2], map_dxt[2];
+  // per-call scratch (grown on demand); maps cached for (k_count, nbp)
+  float* psi[2] = {};  size_t psi_bytes = 0;
+  float* q[2] = {};    size_t q_bytes = 0;
+  float* part = nullptr; size_t part_bytes = 0;
+  int cached_kcount = -1, cached_nbp = -1;
+  CUtensorMap map_psi[2], map_q[2];
+  int* err = nullptr;
+};
+
+}  // namespace ama
+
+using namespace ama;
+
+struct AmaEngine {
+  AxisPlan ax[3];
+  int64_t N = 0;
+  int nk = 0, nspin = 1, nproj = 0, nslots = 0;
+  uint32_t precisions = 0;
+  std::vector<int> npw;
+  std::vector<int64_t> pw_off;
+  int max_npw = 0;
+  int max_rows = 0;
+  DeviceTables d;
+  bool has_potential = false;
+  // workspaces (grown on demand)
+  void* work[2] = {};
+  size_t work_bytes[2] = {};
+  void* ws_proj[2] = {};       // P = psi B^H
+  size_t ws_proj_bytes[2] = {};
+  void* ws_part[2] = {};       // split-K partials
+  size_t ws_part_bytes[2] = {};
+  double* ws_dens = nullptr;   // permuted density accumulator
+  size_t ws_dens_bytes = 0;
+  const void* stage_fn[2][4] = {};  // [prec][stage A, B, C, density B] (grid-specialised)
+  NlTcState tc;
+  bool use_tc = true;
+};
+
+namespace ama {
+int nl_tc_setup(AmaEngine* e);
+int nl_tc_run(AmaEngine* e, int k_first, int k_count, int nbands, const float2* psi, float2* hpsi,
+              cudaStream_t s);
+void nl_tc_free(AmaEngine* e);
+}  // namespace ama
+
+

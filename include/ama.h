@@ -66,6 +66,14 @@ AMA_API int ama_version(void);
 AMA_API int ama_engine_create(const AmaSystemDesc* desc, AmaEngine** engine);
 AMA_API int ama_engine_destroy(AmaEngine* engine);
 
+/* Engine options: option 0 = nonlocal products of the complex64 path on the tensor cores
+ * (value 1, default) or on the SIMT GEMM (value 0). No counterpart in the reference. */
+AMA_API int ama_engine_option(AmaEngine* engine, int32_t option, int32_t value);
+
+/* Device-side status of the tensor-core kernels (0 = fine; otherwise the code of the
+ * first bounded wait that ran out). Synchronous. No counterpart in the reference. */
+AMA_API int ama_tc_status(AmaEngine* engine, int32_t* code);
+
 /* Effective potential V_eff(r) for each spin channel, device FP64 [nspin][n1*n2*n3],
  * natural grid order. Replaces Hamiltonian.__init__ (hamiltonian/operator.py:49-58). */
 AMA_API int ama_set_potential(AmaEngine* engine, const double* v, int32_t nspin, void* stream);
