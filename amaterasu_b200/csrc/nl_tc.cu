@@ -376,8 +376,13 @@ int nl_tc_run(AmaEngine* e, int k_first, int k_count, int nbands, const float2* 
   t.q[1] = t.q[0] + q_half;
   const int kblocks = t.kp / kBK;
   const int mtiles1 = t.p2 / kBM;
+  // Each CTA accumulates at most kChainBlocks k-blocks in tensor memory: the tensor cores
+  // add into the FP32 accumulator with truncation, whose error grows with the chain length;
+  // the split partial sums are then added in FP32 with round-to-nearest by the reduction.
+  constexpr int kChainBlocks = 16;
   int splits = std::max(1, (2 * 148 + mtiles1 * ntile * k_count - 1) / (mtiles1 * ntile * k_count));
-  splits = std::min(splits, std::max(1, kblocks / 8));
+  splits = std::max(splits, (kblocks + kChainBlocks - 1) / kChainBlocks);
+  splits = std::min(splits, kblocks);
   rc = grow(&t.part, &t.part_bytes, (size_t)k_count * splits * nbp * t.p2 * sizeof(float));
   if (rc) return rc;
   if (t.cached_kcount != k_count || t.cached_nbp != nbp || old_psi != t.psi[0] || old_q != t.q[0]) {

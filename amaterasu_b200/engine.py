@@ -100,6 +100,16 @@ class DeviceEngine:
                 pass
             self.handle = None
 
+    def set_tensor_core_nonlocal(self, enabled: bool) -> None:
+        """Route the complex64 projector products to the tcgen05 split-TF32 GEMM (default)
+        or to the SIMT GEMM."""
+        call("ama_engine_option", self.handle, 0, 1 if enabled else 0)
+
+    def tc_status(self) -> int:
+        code = ct.c_int32(0)
+        call("ama_tc_status", self.handle, ct.byref(code))
+        return int(code.value)
+
     def block_offsets(self, nbands: int, k_first: int = 0, k_count: int | None = None):
         """Element offsets of each k's (nbands, npw_k) block in a packed all-k array."""
         k_count = self.nk - k_first if k_count is None else k_count
