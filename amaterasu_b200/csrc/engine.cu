@@ -1059,3 +1059,65 @@ extern "C" int ama_engine_option(AmaEngine* e, int32_t option, int32_t value) {
       return AMA_ERR_ARG;
   }
 }
+
+// ============================================= grid filter without allocation
+// Some callers cannot let a library call cudaMalloc: applications whose device memory is
+// owned by a framework allocator that has already reserved most of the GPU (a cudaMalloc
+// from inside the library then fails or fragments that pool), and latency-sensitive loops
+// in which the implicit device-wide synchronisation of cudaMalloc/cudaFree is not
+// acceptable. For them, ama_grid_filter_noalloc runs the same three-stage filter as
+// ama_grid_filter with its complex work grid in a fixed file-scope device array instead
+// of the lazily grown allocation. The array holds kNoAllocGridPoints complex FP64 values
+// (128^3 points, 32 MiB) and lives on every GPU that loads the library until the process
+// exits. The first call on a device looks up the array's device address
+// (cudaGetSymbolAddress, with that device current); make that first call before any
+// stream capture. Every call shares the array and overwrites it completely before reading
+// it, so nothing needs clearing between calls; calls that overlap on the GPU (different
+// streams, no ordering between them) race on the array.
+namespace {
+constexpr int64_t kNoAllocGridPoints = 128 * 128 * 128;
+__device__ __align__(256) double2 g_noalloc_grid[kNoAllocGridPoints];
+constexpr int kMaxDevices = 64;
+void* g_noalloc_addr[kMaxDevices] = {};
+}  // namespace
+
+extern "C" int ama_grid_filter_noalloc(AmaEngine* e, int32_t slot, int32_t energy_slot, const double* in,
+                                       double* out, double* energy, void* stream) {
+  AMA_REQUIRE(e && in && out, AMA_ERR_ARG, "null argument");
+  AMA_REQUIRE(slot >= 0 && slot < 4 && energy_slot >= -1 && energy_slot < 4, AMA_ERR_ARG, "bad slot");
+  AMA_REQUIRE(e->N <= kNoAllocGridPoints, AMA_ERR_SHAPE,
+              "ama_grid_filter_noalloc: grid of " + std::to_string(e->N) + " points exceeds the fixed work array of " +
+                  std::to_string(kNoAllocGridPoints) + " points (use ama_grid_filter)");
+  auto it = g_filters.find(e);
+  AMA_REQUIRE(it != g_filters.end() && it->second.filt[slot], AMA_ERR_ARG, "filter slot not set");
+  const double* ef = nullptr;
+  if (energy_slot >= 0) {
+    ef = it->second.filt[energy_slot];
+    AMA_REQUIRE(ef && energy, AMA_ERR_ARG, "energy filter slot not set or energy is null");
+  }
+  int dev = 0;
+  AMA_CUDA_TRY(cudaGetDevice(&dev));
+  AMA_REQUIRE(dev >= 0 && dev < kMaxDevices, AMA_ERR_UNSUPPORTED, "device index out of range");
+  if (!g_noalloc_addr[dev]) {
+    void* addr = nullptr;
+    AMA_CUDA_TRY(cudaGetSymbolAddress(&addr, g_noalloc_grid));
+    g_noalloc_addr[dev] = addr;
+  }
+  double2* work = static_cast<double2*>(g_noalloc_addr[dev]);
+  cudaStream_t s = (cudaStream_t)stream;
+  GridView g = grid_view(e);
+  const size_t ps = plane_smem<double>(e), ss = slab_smem<double>(e);
+  AMA_CUDA_TRY(cudaFuncSetAttribute(grid_g1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
+  AMA_CUDA_TRY(cudaFuncSetAttribute(grid_g3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
+  AMA_CUDA_TRY(cudaFuncSetAttribute(grid_g2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
+  auto T = [&](int axis, int dir) { return (const double2*)e->d.tw[AMA_C128][axis][dir]; };
+  const double invN = 1.0 / (double)e->N;
+  grid_g1_kernel<<<g.n1, kFftThreads, ps, s>>>(g, T(1, 1), T(2, 1), in, work);
+  AMA_CHECK_LAUNCH();
+  grid_g2_kernel<<<g.n2, kFftThreads, ss, s>>>(g, T(0, 1), T(0, 0), it->second.filt[slot], ef, invN, invN * invN,
+                                                work, energy);
+  AMA_CHECK_LAUNCH();
+  grid_g3_kernel<<<g.n1, kFftThreads, ps, s>>>(g, T(1, 0), T(2, 0), work, out);
+  AMA_CHECK_LAUNCH();
+  return AMA_OK;
+}

@@ -135,6 +135,17 @@ AMA_API int ama_set_grid_filter(AmaEngine* engine, int32_t slot, const double* f
 AMA_API int ama_grid_filter(AmaEngine* engine, int32_t slot, int32_t energy_slot,
                             const double* in, double* out, double* energy, void* stream);
 
+/* ama_grid_filter without any allocation, for callers that cannot let the library call
+ * cudaMalloc (device memory already reserved by a framework's allocator, or loops that
+ * must not take cudaMalloc's device-wide synchronisation). No counterpart in the
+ * reference. Same arguments and result as ama_grid_filter; the complex work grid is a
+ * fixed device array of 128^3 points (32 MiB, held on every GPU that loads the library),
+ * and a larger grid returns AMA_ERR_SHAPE. The first call on a device looks up the
+ * array's address and should come before any stream capture. All calls share the array:
+ * calls that overlap on the GPU race. */
+AMA_API int ama_grid_filter_noalloc(AmaEngine* engine, int32_t slot, int32_t energy_slot,
+                                    const double* in, double* out, double* energy, void* stream);
+
 /* Forward transform of a real grid field to natural FFT order (device FP64 in
  * [n1*n2*n3], device complex128 out [n1*n2*n3]): out[G] = (1/N) sum_r in(r) e^{-iG.r}.
  * Replaces FFTGrid.to_reciprocal on a density (basis/fft.py:228-235). */
