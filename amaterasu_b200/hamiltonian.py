@@ -82,6 +82,42 @@ class Hamiltonian:
         self._bind()
         return self.engine.hpsi(psi, out, k_first=k_first, k_count=k_count, nbands=nbands, spin=spin)
 
+    def apply_host(self, host_in: torch.Tensor, host_out: torch.Tensor, nbands: int, spin: int = 0, *,
+                   dev_in: torch.Tensor | None = None, dev_out: torch.Tensor | None = None) -> None:
+        """Batched H.psi from host memory to host memory, pipelined over k-points.
+
+        ``host_in``/``host_out`` pack one (nbands, npw_k) block per k (pinned CPU tensors
+        for asynchronous copies). The copy of block k+1 in, the H.psi of block k and the copy
+        of block k-1 out overlap on three streams; the call returns with the work queued on
+        the current stream (synchronise before reading ``host_out``).
+        """
+        eng = self.engine
+        offsets = eng.block_offsets(nbands)
+        if host_in.numel() != int(offsets[-1]) or host_out.numel() != int(offsets[-1]):
+            raise ValueError(f"host blocks hold {host_in.numel()} coefficients, expected {int(offsets[-1])}")
+        dtype = TORCH_DTYPE[self.precision]
+        if dev_in is None:
+            dev_in = torch.empty(host_in.shape, dtype=dtype, device=self.device)
+        if dev_out is None:
+            dev_out = torch.empty_like(dev_in)
+        if not hasattr(self, "_copy_streams"):
+            self._copy_streams = (torch.cuda.Stream(self.device), torch.cuda.Stream(self.device))
+        s_in, s_out = self._copy_streams
+        compute = torch.cuda.current_stream(self.device)
+        s_in.wait_stream(compute)
+        s_out.wait_stream(compute)
+        self._bind()
+        for k in range(eng.nk):
+            a, b = int(offsets[k]), int(offsets[k + 1])
+            with torch.cuda.stream(s_in):
+                dev_in[a:b].copy_(host_in[a:b], non_blocking=True)
+            compute.wait_stream(s_in)
+            eng.hpsi(dev_in[a:b], dev_out[a:b], k_first=k, k_count=1, nbands=nbands, spin=spin)
+            s_out.wait_stream(compute)
+            with torch.cuda.stream(s_out):
+                host_out[a:b].copy_(dev_out[a:b], non_blocking=True)
+        compute.wait_stream(s_out)
+
     def apply_overlap(self, coefficients, ik: int):
         return coefficients
 

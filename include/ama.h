@@ -161,6 +161,11 @@ AMA_API int ama_lda_pz(const double* rho, int64_t npoints, double* eps, double* 
  * Replaces scipy.linalg.eigh in rayleigh_ritz (scf/eigen/subspace.py:74). */
 AMA_API int ama_heev(int32_t n, void* matrices, double* eigenvalues, int32_t batch, void* stream);
 
+/* The same for many small matrices (order n <= 80) at once: one CTA per matrix, cyclic
+ * Jacobi in shared memory, FP64. Used for the per-k-point Rayleigh-Ritz problems of the
+ * batched Davidson (scf/eigen/subspace.py:74 for every k). */
+AMA_API int ama_heev_small(int32_t n, void* matrices, double* eigenvalues, int32_t batch, void* stream);
+
 /* Inverse Cholesky factor of `batch` Hermitian positive-definite FP64 matrices (device,
  * row-major, interleaved complex): on return each holds L^{-1} (lower triangular) with
  * S = L L^H. AMA_ERR_NOT_SPD if a pivot is not positive. Replaces the cholesky +

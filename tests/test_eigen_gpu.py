@@ -86,3 +86,25 @@ def test_solve_dispatch_errors():
         solve("lobpcg", lambda b: b, np.eye(2), np.zeros(2))
     with pytest.raises(NotImplementedError):
         solve("davidson", lambda b: b, np.eye(2), np.zeros(2), apply_overlap=lambda b: b)
+
+
+@pytest.mark.parametrize("n", [1, 2, 7, 20, 33, 80])
+def test_batched_jacobi_matches_eigh(n):
+    """ama_heev_small (one CTA per matrix, cyclic Jacobi) against numpy's eigh."""
+    from amaterasu_b200._lib import call
+    from amaterasu_b200.engine import ptr, stream_ptr
+    rng = np.random.default_rng(n)
+    batch = 5
+    a = rng.normal(size=(batch, n, n)) + 1j * rng.normal(size=(batch, n, n))
+    a = a + np.conj(np.transpose(a, (0, 2, 1)))
+    a[1] = np.diag(np.repeat(np.arange(1, (n + 1) // 2 + 1), 2)[:n]).astype(complex)  # degenerate, already diagonal
+    m = torch.from_numpy(a.copy()).cuda()
+    w = torch.empty((batch, n), dtype=torch.float64, device="cuda")
+    call("ama_heev_small", n, ptr(m), ptr(w), batch, stream_ptr())
+    w = w.cpu().numpy()
+    v = m.cpu().numpy()
+    for b in range(batch):
+        ref = np.linalg.eigvalsh(a[b])
+        np.testing.assert_allclose(w[b], ref, rtol=0, atol=1e-11 * max(1.0, np.abs(ref).max()))
+        np.testing.assert_allclose(v[b].conj().T @ v[b], np.eye(n), atol=1e-12)
+        np.testing.assert_allclose(a[b] @ v[b], v[b] * w[b][None, :], atol=1e-10 * max(1.0, np.abs(ref).max()))
