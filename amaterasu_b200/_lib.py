@@ -66,6 +66,13 @@ SIGNATURES = {
     "ama_heev": (ct.c_int, [_I32, _P, _P, _I32, _P]),
     "ama_potrf_inv": (ct.c_int, [_I32, _P, _I32, _P]),
     "ama_heev_small": (ct.c_int, [_I32, _P, _P, _I32, _P]),
+    "ama_conv3d_fwd_bf16": (ct.c_int, [_P, _P, _P, _P, _I32, _I32, _I32, _I32, _I32, _P]),
+    "ama_conv3d_bwd_data_bf16": (ct.c_int, [_P, _P, _P, _I32, _I32, _I32, _I32, _I32, _P]),
+    "ama_conv3d_bwd_weight_bf16": (ct.c_int, [_P, _P, _P, _P, _I32, _I32, _I32, _I32, _I32, _P]),
+    "ama_silu_fwd_bf16": (ct.c_int, [_P, _P, _I64, _P]),
+    "ama_silu_bwd": (ct.c_int, [_P, _P, _P, _I64, _P]),
+    "ama_upsample2_fwd_bf16": (ct.c_int, [_P, _P, _I64, _I32, _P]),
+    "ama_upsample2_bwd": (ct.c_int, [_P, _P, _I64, _I32, _P]),
 }
 
 _lib = None

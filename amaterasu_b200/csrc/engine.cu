@@ -92,6 +92,7 @@ __device__ __forceinline__ void load_twiddles(C* dst, const C* src, int n) {
 // Grid sizes: compile-time for the engine's common grids (all index arithmetic folds to
 // constants), read from the view otherwise.
 struct DynDims {
+  static constexpr int zsplit = 1;
   template <class V> __device__ static __forceinline__ int n1(const V& v) { return v.n1; }
   template <class V> __device__ static __forceinline__ int a1(const V& v) { return v.A1; }
   template <class V> __device__ static __forceinline__ int n2(const V& v) { return v.n2; }
@@ -100,6 +101,9 @@ struct DynDims {
   template <class V> __device__ static __forceinline__ int a3(const V& v) { return v.A3; }
 };
 template <int N1, int A1, int N2, int A2, int N3, int A3> struct FixDims {
+  // stage B may split each (x, z) slab into z parts (less shared memory per CTA); measured
+  // slower at the benchmark grids, so one part
+  static constexpr int zsplit = 1;
   template <class V> __device__ static constexpr int n1(const V&) { return N1; }
   template <class V> __device__ static constexpr int a1(const V&) { return A1; }
   template <class V> __device__ static constexpr int n2(const V&) { return N2; }
@@ -159,19 +163,20 @@ stage_a_kernel(HpsiView v, const cx_t<T>* __restrict__ tw_y, const cx_t<T>* __re
   for (int i = threadIdx.x; i < plane; i += kFftThreads) dst[i] = pl[i];
 }
 
-// Load the slot rows at one y into an (n1, n3) slab, zero elsewhere, backward x transform.
+// Load the slot rows at one y (columns z0 .. z0+nz-1) into an (n1, nz) slab, zero
+// elsewhere, backward x transform.
 template <typename T, class D>
 __device__ __forceinline__ void slab_load_backward(const HpsiView& v, const cx_t<T>* wb, cx_t<T>* slab,
-                                                   const cx_t<T>* twb) {
+                                                   const cx_t<T>* twb, int nz) {
   using C = cx_t<T>;
   AMA_DIMS(D, v)
-  for (int e = threadIdx.x; e < n1 * n3; e += kFftThreads) {
-    const int x = e / n3, z = e - x * n3;
+  for (int e = threadIdx.x; e < n1 * nz; e += kFftThreads) {
+    const int x = e / nz, z = e - x * nz;
     const int slot = v.slot_of_x[x];
     slab[e] = slot >= 0 ? wb[(int64_t)slot * plane + z] : mk<C>(0, 0);
   }
   __syncthreads();
-  dft_cols<+1>(slab, n1, A1, B1, n3, twb);
+  dft_cols<+1>(slab, n1, A1, B1, nz, twb);
 }
 
 template <typename T, class D>
@@ -180,26 +185,28 @@ stage_b_kernel(HpsiView v, const cx_t<T>* __restrict__ tw_xb, const cx_t<T>* __r
                const T* __restrict__ vpot, cx_t<T>* __restrict__ work) {
   using C = cx_t<T>;
   AMA_DIMS(D, v)
+  constexpr int ZS = D::zsplit;
+  const int nz = n3 / ZS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* slab = reinterpret_cast<C*>(smem_raw);  // [n1][n3]
-  C* twb = slab + n1 * n3;
+  C* slab = reinterpret_cast<C*>(smem_raw);  // [n1][nz]
+  C* twb = slab + n1 * nz;
   C* twf = twb + n1;
-  const int y = blockIdx.x;
+  const int y = blockIdx.x / ZS, z0 = (blockIdx.x - y * ZS) * nz;
   const int gb = blockIdx.y;
   load_tw(twb, tw_xb, n1);
   load_tw(twf, tw_xf, n1);
-  C* wb = work + (int64_t)gb * v.band_elems + (int64_t)y * n3;
-  slab_load_backward<T, D>(v, wb, slab, twb);
-  const T* vy = vpot + (int64_t)y * n3;
-  for (int e = threadIdx.x; e < n1 * n3; e += kFftThreads) {
-    const int x = e / n3, z = e - x * n3;
+  C* wb = work + (int64_t)gb * v.band_elems + (int64_t)y * n3 + z0;
+  slab_load_backward<T, D>(v, wb, slab, twb, nz);
+  const T* vy = vpot + (int64_t)y * n3 + z0;
+  for (int e = threadIdx.x; e < n1 * nz; e += kFftThreads) {
+    const int x = e / nz, z = e - x * nz;
     slab[e] = cscale(slab[e], vy[(int64_t)x * plane + z]);
   }
   __syncthreads();
-  dft_cols<-1>(slab, n1, A1, B1, n3, twf);
-  for (int e = threadIdx.x; e < v.nslots * n3; e += kFftThreads) {
-    const int slot = e / n3, z = e - slot * n3;
-    wb[(int64_t)slot * plane + z] = slab[v.plane_x[slot] * n3 + z];
+  dft_cols<-1>(slab, n1, A1, B1, nz, twf);
+  for (int e = threadIdx.x; e < v.nslots * nz; e += kFftThreads) {
+    const int slot = e / nz, z = e - slot * nz;
+    wb[(int64_t)slot * plane + z] = slab[v.plane_x[slot] * nz + z];
   }
 }
 
@@ -263,7 +270,7 @@ density_b_kernel(HpsiView v, const cx_t<T>* __restrict__ tw_xb, const cx_t<T>* _
   if (weight == 0.0) return;
   load_tw(twb, tw_xb, n1);
   const C* wb = work + (int64_t)gb * v.band_elems + (int64_t)y * n3;
-  slab_load_backward<T, D>(v, wb, slab, twb);
+  slab_load_backward<T, D>(v, wb, slab, twb, n3);
   for (int e = threadIdx.x; e < n1 * n3; e += kFftThreads) {
     const int x = e / n3, z = e - x * n3;
     const C u = slab[e];
@@ -273,22 +280,22 @@ density_b_kernel(HpsiView v, const cx_t<T>* __restrict__ tw_xb, const cx_t<T>* _
 }
 
 template <typename T, class D>
-void fill_stage_table(const void** fn) {
+int fill_stage_table(const void** fn) {
   fn[0] = (const void*)stage_a_kernel<T, D>;
   fn[1] = (const void*)stage_b_kernel<T, D>;
   fn[2] = (const void*)stage_c_kernel<T, D>;
   fn[3] = (const void*)density_b_kernel<T, D>;
+  return D::zsplit;
 }
 
 // Grids with compile-time kernels (cubic cells of the benchmark workloads); any other grid
 // runs the same kernels with sizes read at run time.
 template <typename T>
-void select_stage_table(const AxisPlan* ax, const void** fn) {
+int select_stage_table(const AxisPlan* ax, const void** fn) {
 #define AMA_FIX(N1, A1, N2, A2, N3, A3)                                                         \
   if (ax[0].n == N1 && ax[0].A == A1 && ax[1].n == N2 && ax[1].A == A2 && ax[2].n == N3 &&      \
       ax[2].A == A3) {                                                                           \
-    fill_stage_table<T, FixDims<N1, A1, N2, A2, N3, A3>>(fn);                                   \
-    return;                                                                                      \
+    return fill_stage_table<T, FixDims<N1, A1, N2, A2, N3, A3>>(fn);                            \
   }
   AMA_FIX(20, 5, 20, 5, 20, 5)
   AMA_FIX(25, 5, 25, 5, 25, 5)
@@ -298,7 +305,7 @@ void select_stage_table(const AxisPlan* ax, const void** fn) {
   AMA_FIX(84, 12, 84, 12, 84, 12)
   AMA_FIX(108, 12, 108, 12, 108, 12)
 #undef AMA_FIX
-  fill_stage_table<T, DynDims>(fn);
+  return fill_stage_table<T, DynDims>(fn);
 }
 
 template <typename T>
@@ -393,6 +400,11 @@ template <typename T>
 size_t slab_smem(const AmaEngine* e) {
   return (size_t)(e->ax[0].n * e->ax[2].n + 2 * e->ax[0].n) * sizeof(cx_t<T>);
 }
+template <typename T>
+size_t slab_b_smem(const AmaEngine* e) {
+  const int p = std::is_same<T, float>::value ? AMA_C64 : AMA_C128;
+  return (size_t)(e->ax[0].n * (e->ax[2].n / e->zsplit[p]) + 2 * e->ax[0].n) * sizeof(cx_t<T>);
+}
 
 template <typename T>
 int set_smem_limits(const AmaEngine* e) {
@@ -404,10 +416,10 @@ int set_smem_limits(const AmaEngine* e) {
               "grid plane does not fit in shared memory at this precision");
   const int p = std::is_same<T, float>::value ? AMA_C64 : AMA_C128;
   const void** fn = const_cast<AmaEngine*>(e)->stage_fn[p];
-  select_stage_table<T>(e->ax, fn);
+  const_cast<AmaEngine*>(e)->zsplit[p] = select_stage_table<T>(e->ax, fn);
   AMA_CUDA_TRY(cudaFuncSetAttribute(fn[0], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
   AMA_CUDA_TRY(cudaFuncSetAttribute(fn[2], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
-  AMA_CUDA_TRY(cudaFuncSetAttribute(fn[1], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
+  AMA_CUDA_TRY(cudaFuncSetAttribute(fn[1], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)slab_b_smem<T>(e)));
   AMA_CUDA_TRY(cudaFuncSetAttribute(fn[3], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
   return AMA_OK;
 }
@@ -452,8 +464,8 @@ int hpsi_impl(AmaEngine* e, int k_first, int k_count, int nbands, int spin, cons
 
   rc = run_fft_stages_a<T>(e, v, (int)nb_total, psi, s);
   if (rc) return rc;
-  dim3 gb(e->ax[1].n, nb_total);
-  ((StageBFn<T>)e->stage_fn[p][1])<<<gb, kFftThreads, slab_smem<T>(e), s>>>(
+  dim3 gb(e->ax[1].n * e->zsplit[p], nb_total);
+  ((StageBFn<T>)e->stage_fn[p][1])<<<gb, kFftThreads, slab_b_smem<T>(e), s>>>(
       v, (const C*)e->d.tw[p][0][0], (const C*)e->d.tw[p][0][1], vpot, (C*)e->work[p]);
   AMA_CHECK_LAUNCH();
   dim3 gc(e->nslots, nb_total);
@@ -833,7 +845,7 @@ GridView grid_view(const AmaEngine* e) {
   return g;
 }
 
-__global__ void grid_g1_kernel(GridView g, const double2* tw_y, const double2* tw_z,
+__global__ void __launch_bounds__(kFftThreads) grid_g1_kernel(GridView g, const double2* tw_y, const double2* tw_z,
                                const double* __restrict__ in, double2* __restrict__ work) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double2* plane = reinterpret_cast<double2*>(smem_raw);
@@ -853,7 +865,7 @@ __global__ void grid_g1_kernel(GridView g, const double2* tw_y, const double2* t
   for (int64_t i = threadIdx.x; i < g.plane_elems; i += blockDim.x) dst[i] = plane[i];
 }
 
-__global__ void grid_g2_kernel(GridView g, const double2* tw_f, const double2* tw_b,
+__global__ void __launch_bounds__(kFftThreads) grid_g2_kernel(GridView g, const double2* tw_f, const double2* tw_b,
                                const double* __restrict__ filt, const double* __restrict__ efilt,
                                double scale, double escale, double2* __restrict__ work,
                                double* __restrict__ energy) {
@@ -901,7 +913,7 @@ __global__ void grid_g2_kernel(GridView g, const double2* tw_f, const double2* t
   }
 }
 
-__global__ void grid_g3_kernel(GridView g, const double2* tw_y, const double2* tw_z,
+__global__ void __launch_bounds__(kFftThreads) grid_g3_kernel(GridView g, const double2* tw_y, const double2* tw_z,
                                const double2* __restrict__ work, double* __restrict__ out) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double2* plane = reinterpret_cast<double2*>(smem_raw);
@@ -926,7 +938,7 @@ __global__ void grid_g3_kernel(GridView g, const double2* tw_y, const double2* t
 namespace {
 // Forward x transform of the G1 output and scatter to natural (x, y, z) order with 1/N:
 // out[G] = (1/N) sum_r in(r) e^{-iG.r}.
-__global__ void grid_g2f_kernel(GridView g, const double2* tw_f, const double2* __restrict__ work,
+__global__ void __launch_bounds__(kFftThreads) grid_g2f_kernel(GridView g, const double2* tw_f, const double2* __restrict__ work,
                                 double2* __restrict__ out, double scale) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double2* slab = reinterpret_cast<double2*>(smem_raw);

@@ -72,6 +72,7 @@ struct AmaEngine {
   double* ws_dens = nullptr;   // permuted density accumulator
   size_t ws_dens_bytes = 0;
   const void* stage_fn[2][4] = {};  // [prec][stage A, B, C, density B] (grid-specialised)
+  int zsplit[2] = {1, 1};           // [prec] z halves per stage-B slab
   NlTcState tc;
   bool use_tc = true;
 };

@@ -248,16 +248,36 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap a_hi, const __grid_constant__
       }
     }
   } else if (have) {
+    // hpsi[m][row] += D[row][m]: 32 columns per round so that 32 independent loads of the
+    // FFT result are in flight per thread before the adds and stores.
     const int k = p.k_first + kl;
     const int ld = 2 * p.npw[k];
-    float* outk = p.out + 2 * (p.pw_off[k] - p.pw_off[p.k_first]) * p.nbands;
-    for (int c0 = 0; c0 < p.bn; c0 += 8) {
-      float v[8];
-      tmem_ld8(trow + c0, v);
+    float* __restrict__ outk = p.out + 2 * (p.pw_off[k] - p.pw_off[p.k_first]) * p.nbands;
+    const bool row_ok = row < ld;
+    for (int c0 = 0; c0 < p.bn; c0 += 32) {
+      float v[32];
 #pragma unroll
-      for (int t = 0; t < 8; ++t) {
+      for (int q = 0; q < 4; ++q) {
+        float w[8];
+        if (c0 + 8 * q < p.bn) {
+          tmem_ld8(trow + c0 + 8 * q, w);
+        } else {
+#pragma unroll
+          for (int t = 0; t < 8; ++t) w[t] = 0.f;
+        }
+#pragma unroll
+        for (int t = 0; t < 8; ++t) v[8 * q + t] = w[t];
+      }
+      float old[32];
+#pragma unroll
+      for (int t = 0; t < 32; ++t) {
         const int m = nt * p.bn + c0 + t;
-        if (m < p.n_valid && row < ld) outk[(int64_t)m * ld + row] += v[t];
+        old[t] = (row_ok && c0 + t < p.bn && m < p.n_valid) ? outk[(int64_t)m * ld + row] : 0.f;
+      }
+#pragma unroll
+      for (int t = 0; t < 32; ++t) {
+        const int m = nt * p.bn + c0 + t;
+        if (row_ok && c0 + t < p.bn && m < p.n_valid) outk[(int64_t)m * ld + row] = old[t] + v[t];
       }
     }
   }

@@ -172,6 +172,22 @@ AMA_API int ama_heev_small(int32_t n, void* matrices, double* eigenvalues, int32
  * solve_triangular pair of orthonormalize (scf/eigen/subspace.py:17-32). */
 AMA_API int ama_potrf_inv(int32_t n, void* matrices, int32_t batch, void* stream);
 
+/* ---- learned start density: periodic 3D convolution network (no counterpart in the
+ * reference; the start density it replaces is hamiltonian/local.py:77-106).
+ * Tensors [batch][channels][d][d][d], 3x3x3 kernels w[co][ci][3][3][3], circular
+ * padding 1, stride 1 or 2 (d_out = d_in / stride); BF16 activations and weights
+ * (x, w, y of the _bf16 functions), FP32 accumulation, outputs and gradients. */
+AMA_API int ama_conv3d_fwd_bf16(const void* x, const void* w, const float* bias, float* y, int32_t batch,
+                                int32_t ci, int32_t co, int32_t din, int32_t stride, void* stream);
+AMA_API int ama_conv3d_bwd_data_bf16(const float* dy, const void* w, float* dx, int32_t batch, int32_t ci,
+                                     int32_t co, int32_t din, int32_t stride, void* stream);
+AMA_API int ama_conv3d_bwd_weight_bf16(const float* dy, const void* x, float* dw, float* dbias, int32_t batch,
+                                       int32_t ci, int32_t co, int32_t din, int32_t stride, void* stream);
+AMA_API int ama_silu_fwd_bf16(const float* x, void* y, int64_t n, void* stream);
+AMA_API int ama_silu_bwd(const float* x, const float* dy, float* dx, int64_t n, void* stream);
+AMA_API int ama_upsample2_fwd_bf16(const void* x, void* y, int64_t channels, int32_t d, void* stream);
+AMA_API int ama_upsample2_bwd(const float* dy, float* dx, int64_t channels, int32_t d, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
