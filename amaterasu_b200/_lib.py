@@ -26,6 +26,11 @@ class NotConvergedError(AmaError):
     pass
 
 
+class AmaKOperand(ct.Structure):
+    _fields_ = [("base", ct.c_void_p), ("rows_per_k", ct.c_int64), ("row0", ct.c_int64),
+                ("ragged", ct.c_int32), ("ld", ct.c_int64), ("kstride", ct.c_int64)]
+
+
 class AmaSystemDesc(ct.Structure):
     _fields_ = [
         ("n1", ct.c_int32), ("n2", ct.c_int32), ("n3", ct.c_int32),
@@ -59,6 +64,10 @@ SIGNATURES = {
                              _P, _P, _I64, _I64, _I32, _P]),
     "ama_residual_precondition": (ct.c_int, [_I32, _I32, _I32, _P, _P, _P, _P, _P, _P, _I32, _P, _P]),
     "ama_lda_pz": (ct.c_int, [_P, _I64, _P, _P, _P]),
+    "ama_kbatch_zgemm": (ct.c_int, [_I32, _I32, _I32, _I32, _I32, _I32, _P, _P, _P, _P, _P, _P, _P, _I32, _I32,
+                                    _P]),
+    "ama_kbatch_residual": (ct.c_int, [_I32, _I32, _I32, _P, _P, _P, _P, _P, _P, _P, _P, _I32, _P, _P]),
+    "ama_kbatch_copy_rows": (ct.c_int, [_I32, _I32, _I32, _P, _P, _P, _I64, _I64, _P, _I64, _I64, _P]),
     "ama_set_grid_filter": (ct.c_int, [_P, _I32, _P]),
     "ama_grid_filter": (ct.c_int, [_P, _I32, _I32, _P, _P, _P, _P]),
     "ama_grid_fft_forward": (ct.c_int, [_P, _P, _P, _P]),

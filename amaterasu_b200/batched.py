@@ -1,0 +1,200 @@
+"""Block Davidson for every k-point at once (lockstep), on per-k packed device storage.
+
+Per k-point this is the reference's algorithm (amaterasu ``scf/eigen/davidson.py:48-111``:
+Rayleigh-Ritz, residuals, Teter-Payne-Allan corrections of the active bands, two
+projections off the basis, drop directions below 1e-7, orthonormalise, extend, collapse at
+subspace_factor * nbands). All k-points advance together: every step is one launch over all
+k (ragged plane-wave counts), H.psi runs on every k's new block in one engine call, the
+small per-k problems are solved by the batched Jacobi eigensolver, and the host synchronises
+three times per iteration for the whole set instead of per k.
+
+Storage: the basis of k-point k is a (cap, npw_k) block at cap * pw_off[k]; every k carries
+the same number of rows. When a k-point has fewer new directions than the others (fewer
+active bands, or directions dropped as dependent), its surplus rows are zero and marked
+invalid: their Rayleigh-Ritz diagonal is set far above the spectrum, which decouples them.
+Orthonormalisation (initial block and new directions) uses the Gram eigendecomposition,
+which spans the same space as the reference's Cholesky/SVD, so the Ritz pairs agree.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+
+import numpy as np
+import torch
+
+from ._lib import AMA_C64, AMA_C128, AmaKOperand, call
+from .engine import engine_for, ptr, stream_ptr
+
+_BIG = 1.0e6          # Ha, diagonal of invalid Rayleigh-Ritz rows
+_JACOBI_MAX = 80
+
+
+class _KOp:
+    """An operand inside per-k packed storage."""
+
+    def __init__(self, t: torch.Tensor, rows_per_k=0, row0=0, ragged=True, ld=0, kstride=0):
+        self.t = t
+        self.c = AmaKOperand(ct.c_void_p(t.data_ptr()), int(rows_per_k), int(row0), 1 if ragged else 0,
+                             int(ld), int(kstride))
+
+
+class BatchedDavidson:
+    def __init__(self, system, nbands: int, dtype=torch.complex128):
+        self.eng = engine_for(system)
+        self.system = system
+        self.nk = self.eng.nk
+        self.nb = nbands
+        self.dtype = dtype
+        self.prec = AMA_C64 if dtype == torch.complex64 else AMA_C128
+        dev = self.eng.device
+        self.dev = dev
+        self.npw = torch.from_numpy(self.eng.npw.astype(np.int32)).to(dev)
+        self.pw_off = torch.from_numpy(self.eng.pw_off[:-1].astype(np.int64)).to(dev)
+        self.max_npw = int(self.eng.npw.max())
+        self.total_pw = int(self.eng.pw_off[-1])
+        self.kin = torch.from_numpy(np.concatenate([s.kinetic_energy for s in system.wave_spheres])).to(dev)
+        self.max_sub = min(4 * nbands, int(self.eng.npw.min()))
+        self.cap = self.max_sub + nbands
+
+    # ---------------------------------------------------------------- kernels
+    def _gemm(self, form, m, n, k, a: _KOp, b: _KOp, c: _KOp, alpha=1.0, beta=0.0, max_m=None, max_n=None):
+        al = (ct.c_double * 2)(float(np.real(alpha)), float(np.imag(alpha)))
+        be = (ct.c_double * 2)(float(np.real(beta)), float(np.imag(beta)))
+        mm = max_m if max_m is not None else (self.max_npw if m < 0 else m)
+        nn = max_n if max_n is not None else (self.max_npw if n < 0 else n)
+        call("ama_kbatch_zgemm", self.prec, form, self.nk, m, n, k, ptr(self.npw), ptr(self.pw_off),
+             ct.byref(a.c), ct.byref(b.c), ct.byref(c.c), al, be, mm, nn, stream_ptr())
+
+    def _blocks(self, rows):
+        return torch.zeros(rows * self.total_pw, dtype=self.dtype, device=self.dev)
+
+    def _small(self, rows, cols):
+        return torch.zeros((self.nk, rows, cols), dtype=self.dtype, device=self.dev)
+
+    def _gram(self, blk: torch.Tensor, rows: int, rows_per_k: int, row0: int = 0) -> torch.Tensor:
+        """G[k] = X_k X_k^H for `rows` rows of a packed block (FP64, Hermitised)."""
+        g = self._small(rows, rows)
+        op = _KOp(blk, rows_per_k, row0)
+        self._gemm(1, rows, rows, -1, op, op, _KOp(g, ragged=False, ld=rows, kstride=rows * rows))
+        g = g.to(torch.complex128)
+        return 0.5 * (g + g.conj().transpose(1, 2))
+
+    def _heev(self, mats: torch.Tensor):
+        """Batched FP64 Hermitian eigensolve: (w ascending [nk][n], V columns [nk][n][n])."""
+        n = mats.shape[1]
+        m = mats.contiguous().clone()
+        w = torch.empty((self.nk, n), dtype=torch.float64, device=self.dev)
+        if n <= _JACOBI_MAX:
+            call("ama_heev_small", n, ptr(m), ptr(w), self.nk, stream_ptr())
+        else:
+            call("ama_heev", n, ptr(m), ptr(w), self.nk, stream_ptr())
+        return w, m
+
+    def _rotate(self, rot: torch.Tensor, src: torch.Tensor, src_rows_per_k: int, k_rows: int, out_rows: int):
+        """out[k] = rot[k] (out_rows x k_rows) . src[k][:k_rows]  -> packed (out_rows, npw_k)."""
+        out = self._blocks(out_rows)
+        r = rot.to(self.dtype).contiguous()
+        self._gemm(0, out_rows, -1, k_rows, _KOp(r, ragged=False, ld=k_rows, kstride=out_rows * k_rows),
+                   _KOp(src, src_rows_per_k, 0), _KOp(out, out_rows, 0))
+        return out
+
+    def _copy(self, src, src_rows_per_k, src_row0, dst, dst_rows_per_k, dst_row0, nrows):
+        call("ama_kbatch_copy_rows", self.prec, self.nk, nrows, ptr(self.npw), ptr(self.pw_off), ptr(src),
+             src_rows_per_k, src_row0, ptr(dst), dst_rows_per_k, dst_row0, stream_ptr())
+
+    def _orthonormal_rows(self, blk: torch.Tensor, rows: int, threshold: float, drop_small: bool):
+        """Orthonormal rows spanning the dominant part of each k's block (Gram eigh),
+        zero rows where directions are dropped. Returns (block, valid [nk][rows] numpy)."""
+        g = self._gram(blk, rows, rows)
+        if drop_small:  # rows whose norm is <= threshold are removed before the SVD
+            diag = torch.diagonal(g, dim1=1, dim2=2).real
+            small = diag <= threshold * threshold
+            g = g * (~small)[:, :, None] * (~small)[:, None, :]
+        w, u = self._heev(g)
+        s = torch.sqrt(torch.clamp(w, min=0.0))
+        smax = s.max(dim=1, keepdim=True).values
+        keep = s > threshold * torch.clamp(smax, min=1e-300)
+        inv = torch.where(keep, 1.0 / torch.where(keep, s, torch.ones_like(s)), torch.zeros_like(s))
+        rot = (u.conj().transpose(1, 2) * inv[:, :, None])  # rows: u_j^H / s_j
+        out = self._rotate(rot, blk, rows, rows, rows)
+        return out, keep.cpu().numpy()
+
+    def _rr(self, B, HB, m, valid):
+        p = self._small(m, m)
+        self._gemm(1, m, m, -1, _KOp(B, self.cap, 0), _KOp(HB, self.cap, 0),
+                   _KOp(p, ragged=False, ld=m, kstride=m * m))
+        p = p.to(torch.complex128).conj()
+        p = 0.5 * (p + p.conj().transpose(1, 2))
+        inval = torch.from_numpy(~valid[:, :m]).to(self.dev)
+        p = p * (~inval)[:, :, None] * (~inval)[:, None, :]
+        p = p + torch.diag_embed(inval.to(torch.float64) * _BIG).to(torch.complex128)
+        w, v = self._heev(p)
+        rot = v[:, :, :self.nb].transpose(1, 2)  # (nb x m) per k: X_n = sum_i V[i, n] b_i
+        X = self._rotate(rot, B, self.cap, m, self.nb)
+        HX = self._rotate(rot, HB, self.cap, m, self.nb)
+        return w[:, :self.nb].contiguous(), X, HX
+
+    def _apply(self, H, blk, rows, spin):
+        out = torch.empty_like(blk)
+        self.eng.hpsi(blk, out, k_first=0, k_count=self.nk, nbands=rows, spin=spin)
+        return out
+
+    # -------------------------------------------------------------------- run
+    def run(self, H, guess_packed: torch.Tensor, *, tolerance=1e-8, max_iterations=40, spin=0):
+        """Lowest nbands eigenpairs at every k. ``guess_packed`` packs one (nbands, npw_k)
+        block per k; returns (eigenvalues [nk][nb] numpy, X packed, norms numpy, iterations)."""
+        nb, cap = self.nb, self.cap
+        H._bind()
+        X0, ok = self._orthonormal_rows(guess_packed.to(self.dtype).contiguous(), nb, 1e-10, False)
+        if not ok.all():
+            raise ValueError("the starting block of some k-point is rank deficient")
+        B, HB = self._blocks(cap), self._blocks(cap)
+        HX0 = self._apply(H, X0, nb, spin)
+        self._copy(X0, nb, 0, B, cap, 0, nb)
+        self._copy(HX0, nb, 0, HB, cap, 0, nb)
+        valid = np.zeros((self.nk, cap), dtype=bool)
+        valid[:, :nb] = True
+        m = nb
+        eps, X, HX = self._rr(B, HB, m, valid)
+        norms = np.full((self.nk, nb), np.inf)
+        it = 0
+        for it in range(1, max_iterations + 1):
+            nrm = torch.empty((self.nk, nb), dtype=torch.float64, device=self.dev)
+            call("ama_kbatch_residual", self.prec, self.nk, nb, ptr(self.npw), ptr(self.pw_off), ptr(X), ptr(HX),
+                 ptr(eps), ptr(self.kin), ptr(nrm), None, 0, None, stream_ptr())
+            norms = nrm.cpu().numpy()
+            active = norms > tolerance
+            counts = active.sum(axis=1)
+            nn = int(counts.max())
+            if nn == 0:
+                break
+            rows = np.full((self.nk, nb), -1, dtype=np.int32)
+            for k in range(self.nk):
+                idx = np.nonzero(active[k])[0]
+                rows[k, idx] = np.arange(len(idx), dtype=np.int32)
+            rows_t = torch.from_numpy(rows).to(self.dev)
+            C = self._blocks(nn)
+            call("ama_kbatch_residual", self.prec, self.nk, nb, ptr(self.npw), ptr(self.pw_off), ptr(X), ptr(HX),
+                 ptr(eps), ptr(self.kin), ptr(nrm), ptr(rows_t), nn, ptr(C), stream_ptr())
+            for _ in range(2):
+                t = self._small(nn, m)
+                self._gemm(1, nn, m, -1, _KOp(C, nn, 0), _KOp(B, cap, 0), _KOp(t, ragged=False, ld=m, kstride=nn * m))
+                self._gemm(0, nn, -1, m, _KOp(t, ragged=False, ld=m, kstride=nn * m), _KOp(B, cap, 0), _KOp(C, nn, 0),
+                           alpha=-1.0, beta=1.0)
+            new, keep1 = self._orthonormal_rows(C, nn, 1e-7, True)
+            if not keep1.any():
+                break
+            new, keep = self._orthonormal_rows(new, nn, 0.5, False)
+            HN = self._apply(H, new, nn, spin)
+            self._copy(new, nn, 0, B, cap, m, nn)
+            self._copy(HN, nn, 0, HB, cap, m, nn)
+            valid[:, m:m + nn] = keep
+            m += nn
+            eps, X, HX = self._rr(B, HB, m, valid)
+            if m + nb > self.max_sub:
+                self._copy(X, nb, 0, B, cap, 0, nb)
+                self._copy(HX, nb, 0, HB, cap, 0, nb)
+                valid[:] = False
+                valid[:, :nb] = True
+                m = nb
+        return eps.cpu().numpy(), X, norms, it

@@ -210,6 +210,85 @@ stage_b_kernel(HpsiView v, const cx_t<T>* __restrict__ tw_xb, const cx_t<T>* __r
   }
 }
 
+// Stage B with each x column held in registers (complex64, compile-time n1): one thread
+// per (y, z) column of a band, no shared memory. The backward transform (natural x in,
+// permuted out), the V multiply and the forward transform (permuted in, natural out) are
+// the same four-step DFTs as the shared-memory passes, done on a register array.
+constexpr int kRegBThreads = 128;
+
+template <int N, int A, int S, bool NAT_IN>
+__device__ __forceinline__ void dft_line_reg(float2 (&v)[N], const float2* __restrict__ tw) {
+  constexpr int B = N / A;
+  if constexpr (NAT_IN) {
+    static_for<B>([&](auto bb) {
+      constexpr int b = decltype(bb)::value;
+      float2 t[A];
+      static_for<A>([&](auto aa) { t[decltype(aa)::value] = v[decltype(aa)::value * B + b]; });
+      dft_reg<A, S>(t);
+      static_for<A>([&](auto cc) {
+        constexpr int c = decltype(cc)::value;
+        if constexpr (b * c % N != 0) t[c] = cmul(t[c], __ldg(tw + (b * c) % N));
+        v[c * B + b] = t[c];
+      });
+    });
+    static_for<A>([&](auto cc) {
+      constexpr int c = decltype(cc)::value;
+      float2 t[B];
+      static_for<B>([&](auto dd) { t[decltype(dd)::value] = v[c * B + decltype(dd)::value]; });
+      dft_reg<B, S>(t);
+      static_for<B>([&](auto dd) { v[c * B + decltype(dd)::value] = t[decltype(dd)::value]; });
+    });
+  } else {
+    static_for<A>([&](auto cc) {
+      constexpr int c = decltype(cc)::value;
+      float2 t[B];
+      static_for<B>([&](auto dd) { t[decltype(dd)::value] = v[c * B + decltype(dd)::value]; });
+      dft_reg<B, S>(t);
+      static_for<B>([&](auto ee) {
+        constexpr int e = decltype(ee)::value;
+        if constexpr (c * e % N != 0) t[e] = cmul(t[e], __ldg(tw + (c * e) % N));
+        v[c * B + e] = t[e];
+      });
+    });
+    static_for<B>([&](auto ee) {
+      constexpr int e = decltype(ee)::value;
+      float2 t[A];
+      static_for<A>([&](auto cc) { t[decltype(cc)::value] = v[decltype(cc)::value * B + e]; });
+      dft_reg<A, S>(t);
+      static_for<A>([&](auto gg) { v[decltype(gg)::value * B + e] = t[decltype(gg)::value]; });
+    });
+  }
+}
+
+template <int NX, int AX, class D>
+__global__ void __launch_bounds__(kRegBThreads)
+stage_b_reg_kernel(HpsiView v, const float2* __restrict__ tw_xb, const float2* __restrict__ tw_xf,
+                   const float* __restrict__ vpot, float2* __restrict__ work) {
+  AMA_DIMS(D, v)
+  const int col = blockIdx.x * kRegBThreads + threadIdx.x;  // y * n3 + z
+  if (col >= plane) return;
+  float2* wb = work + (int64_t)blockIdx.y * v.band_elems + col;
+  float2 r[NX];
+  static_for<NX>([&](auto xx) {
+    constexpr int x = decltype(xx)::value;
+    const int slot = __ldg(v.slot_of_x + x);
+    r[x] = slot >= 0 ? wb[(int64_t)slot * plane] : make_float2(0.f, 0.f);
+  });
+  dft_line_reg<NX, AX, +1, true>(r, tw_xb);
+  static_for<NX>([&](auto pp) {
+    constexpr int p = decltype(pp)::value;
+    const float s = __ldg(vpot + (int64_t)p * plane + col);
+    r[p].x *= s;
+    r[p].y *= s;
+  });
+  dft_line_reg<NX, AX, -1, false>(r, tw_xf);
+  static_for<NX>([&](auto xx) {
+    constexpr int x = decltype(xx)::value;
+    const int slot = __ldg(v.slot_of_x + x);
+    if (slot >= 0) wb[(int64_t)slot * plane] = r[x];
+  });
+}
+
 template <typename T, class D>
 __global__ void __launch_bounds__(kFftThreads)
 stage_c_kernel(HpsiView v, const cx_t<T>* __restrict__ tw_y, const cx_t<T>* __restrict__ tw_z,
@@ -279,23 +358,38 @@ density_b_kernel(HpsiView v, const cx_t<T>* __restrict__ tw_xb, const cx_t<T>* _
   }
 }
 
+struct StageInfo { int zsplit; bool regb; };
+
 template <typename T, class D>
-int fill_stage_table(const void** fn) {
+StageInfo fill_stage_table(const void** fn) {
   fn[0] = (const void*)stage_a_kernel<T, D>;
   fn[1] = (const void*)stage_b_kernel<T, D>;
   fn[2] = (const void*)stage_c_kernel<T, D>;
   fn[3] = (const void*)density_b_kernel<T, D>;
-  return D::zsplit;
+  return {D::zsplit, false};
+}
+
+// complex64 on a compile-time grid with short x columns: register-resident stage B
+template <int N1, int A1, class D>
+StageInfo fill_stage_table_reg(const void** fn) {
+  StageInfo info = fill_stage_table<float, D>(fn);
+  fn[1] = (const void*)stage_b_reg_kernel<N1, A1, D>;
+  info.regb = true;
+  return info;
 }
 
 // Grids with compile-time kernels (cubic cells of the benchmark workloads); any other grid
 // runs the same kernels with sizes read at run time.
 template <typename T>
-int select_stage_table(const AxisPlan* ax, const void** fn) {
+StageInfo select_stage_table(const AxisPlan* ax, const void** fn) {
 #define AMA_FIX(N1, A1, N2, A2, N3, A3)                                                         \
   if (ax[0].n == N1 && ax[0].A == A1 && ax[1].n == N2 && ax[1].A == A2 && ax[2].n == N3 &&      \
       ax[2].A == A3) {                                                                           \
-    return fill_stage_table<T, FixDims<N1, A1, N2, A2, N3, A3>>(fn);                            \
+    using D = FixDims<N1, A1, N2, A2, N3, A3>;                                                   \
+    if constexpr (std::is_same<T, float>::value && N1 <= 96)                                     \
+      return fill_stage_table_reg<N1, A1, D>(fn);                                                \
+    else                                                                                         \
+      return fill_stage_table<T, D>(fn);                                                         \
   }
   AMA_FIX(20, 5, 20, 5, 20, 5)
   AMA_FIX(25, 5, 25, 5, 25, 5)
@@ -416,10 +510,13 @@ int set_smem_limits(const AmaEngine* e) {
               "grid plane does not fit in shared memory at this precision");
   const int p = std::is_same<T, float>::value ? AMA_C64 : AMA_C128;
   const void** fn = const_cast<AmaEngine*>(e)->stage_fn[p];
-  const_cast<AmaEngine*>(e)->zsplit[p] = select_stage_table<T>(e->ax, fn);
+  const StageInfo info = select_stage_table<T>(e->ax, fn);
+  const_cast<AmaEngine*>(e)->zsplit[p] = info.zsplit;
+  const_cast<AmaEngine*>(e)->regb[p] = info.regb;
   AMA_CUDA_TRY(cudaFuncSetAttribute(fn[0], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
   AMA_CUDA_TRY(cudaFuncSetAttribute(fn[2], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
-  AMA_CUDA_TRY(cudaFuncSetAttribute(fn[1], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)slab_b_smem<T>(e)));
+  if (!info.regb)
+    AMA_CUDA_TRY(cudaFuncSetAttribute(fn[1], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)slab_b_smem<T>(e)));
   AMA_CUDA_TRY(cudaFuncSetAttribute(fn[3], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
   return AMA_OK;
 }
@@ -464,9 +561,15 @@ int hpsi_impl(AmaEngine* e, int k_first, int k_count, int nbands, int spin, cons
 
   rc = run_fft_stages_a<T>(e, v, (int)nb_total, psi, s);
   if (rc) return rc;
-  dim3 gb(e->ax[1].n * e->zsplit[p], nb_total);
-  ((StageBFn<T>)e->stage_fn[p][1])<<<gb, kFftThreads, slab_b_smem<T>(e), s>>>(
+  if (e->regb[p]) {
+    dim3 gr((e->ax[1].n * e->ax[2].n + kRegBThreads - 1) / kRegBThreads, nb_total);
+    ((StageBFn<T>)e->stage_fn[p][1])<<<gr, kRegBThreads, 0, s>>>(
+        v, (const C*)e->d.tw[p][0][0], (const C*)e->d.tw[p][0][1], vpot, (C*)e->work[p]);
+  } else {
+    dim3 gb(e->ax[1].n * e->zsplit[p], nb_total);
+    ((StageBFn<T>)e->stage_fn[p][1])<<<gb, kFftThreads, slab_b_smem<T>(e), s>>>(
       v, (const C*)e->d.tw[p][0][0], (const C*)e->d.tw[p][0][1], vpot, (C*)e->work[p]);
+  }
   AMA_CHECK_LAUNCH();
   dim3 gc(e->nslots, nb_total);
   ((StageCFn<T>)e->stage_fn[p][2])<<<gc, kFftThreads, plane_smem<T>(e), s>>>(

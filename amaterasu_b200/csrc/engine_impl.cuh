@@ -73,6 +73,7 @@ struct AmaEngine {
   size_t ws_dens_bytes = 0;
   const void* stage_fn[2][4] = {};  // [prec][stage A, B, C, density B] (grid-specialised)
   int zsplit[2] = {1, 1};           // [prec] z halves per stage-B slab
+  bool regb[2] = {false, false};    // [prec] stage B with register-resident x columns
   NlTcState tc;
   bool use_tc = true;
 };

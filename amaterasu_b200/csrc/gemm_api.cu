@@ -67,3 +67,83 @@ extern "C" int ama_zgemm(int32_t precision, int32_t trans_b, int32_t m, int32_t 
              ? zgemm_impl<float>(trans_b, m, n, k, alpha, a, lda, stride_a, b, ldb, stride_b, beta, c, ldc, stride_c, batch, s)
              : zgemm_impl<double>(trans_b, m, n, k, alpha, a, lda, stride_a, b, ldb, stride_b, beta, c, ldc, stride_c, batch, s);
 }
+
+// ------------------------------------------------------------ per-k ragged batches
+// One GEMM per k-point in one launch; any of m, n, k may be the k-point's plane-wave
+// count (passed as -1). Operands live in packed per-k blocks (see AmaKOperand in ama.h).
+namespace {
+
+struct KOp {
+  char* base;
+  int64_t rows_per_k, row0, ld, kstride;
+  int32_t ragged;
+};
+
+template <typename C> struct KBatch {
+  KOp a, b, c;
+  int m, n, k;
+  const int* npw;
+  const int64_t* pw_off;
+  __device__ const C* at(const KOp& o, int z, int np, int64_t po) const {
+    int64_t off;
+    if (o.ragged) off = o.rows_per_k * po + o.row0 * np;
+    else off = z * o.kstride + o.row0 * o.ld;
+    return reinterpret_cast<const C*>(o.base) + off;
+  }
+  __device__ GemmProblem<C> operator()(int z) const {
+    const int np = npw[z];
+    const int64_t po = pw_off[z];
+    GemmProblem<C> p;
+    p.a = at(a, z, np, po);
+    p.b = at(b, z, np, po);
+    p.c = const_cast<C*>(at(c, z, np, po));
+    p.m = m < 0 ? np : m;
+    p.n = n < 0 ? np : n;
+    p.k = k < 0 ? np : k;
+    p.lda = a.ragged ? np : a.ld;
+    p.ldb = b.ragged ? np : b.ld;
+    p.ldc = c.ragged ? np : c.ld;
+    return p;
+  }
+};
+
+KOp to_kop(const AmaKOperand* o) {
+  KOp r;
+  r.base = (char*)o->base;
+  r.rows_per_k = o->rows_per_k;
+  r.row0 = o->row0;
+  r.ld = o->ld;
+  r.kstride = o->kstride;
+  r.ragged = o->ragged;
+  return r;
+}
+
+template <typename T>
+int kbatch_impl(int form, int nk, int m, int n, int k, const int32_t* npw, const int64_t* pw_off,
+                const AmaKOperand* a, const AmaKOperand* b, const AmaKOperand* c, const double* alpha,
+                const double* beta, int max_m, int max_n, cudaStream_t s) {
+  using C = cx_t<T>;
+  KBatch<C> kb{to_kop(a), to_kop(b), to_kop(c), m, n, k, npw, pw_off};
+  const C al = mk<C>(alpha[0], alpha[1]), be = mk<C>(beta[0], beta[1]);
+  cudaError_t err;
+  if (form == 0) err = launch_cgemm<T, kNN>(kb, nk, max_m, max_n, 1, al, be, (C*)nullptr, 0, s);
+  else if (form == 1) err = launch_cgemm<T, kNC>(kb, nk, max_m, max_n, 1, al, be, (C*)nullptr, 0, s);
+  else err = launch_cgemm<T, kCN>(kb, nk, max_m, max_n, 1, al, be, (C*)nullptr, 0, s);
+  AMA_CUDA_TRY(err);
+  return AMA_OK;
+}
+
+}  // namespace
+
+extern "C" int ama_kbatch_zgemm(int32_t precision, int32_t form, int32_t nk, int32_t m, int32_t n, int32_t k,
+                                const int32_t* npw, const int64_t* pw_off, const AmaKOperand* a,
+                                const AmaKOperand* b, const AmaKOperand* c, const double* alpha,
+                                const double* beta, int32_t max_m, int32_t max_n, void* stream) {
+  AMA_REQUIRE(precision == AMA_C64 || precision == AMA_C128, AMA_ERR_ARG, "bad precision");
+  AMA_REQUIRE(form >= 0 && form <= 2, AMA_ERR_ARG, "form must be 0, 1 or 2");
+  AMA_REQUIRE(a && b && c && npw && pw_off && alpha && beta, AMA_ERR_ARG, "null argument");
+  AMA_REQUIRE(nk >= 1 && max_m >= 1 && max_n >= 1, AMA_ERR_SHAPE, "bad sizes");
+  cudaStream_t s = (cudaStream_t)stream;
+  return precision == AMA_C64 ? kbatch_impl<float>(form, nk, m, n, k, npw, pw_off, a, b, c, alpha, beta, max_m, max_n, s)
+                              : kbatch_impl<double>(form, nk, m, n, k, npw, pw_off, a, b, c, alpha, beta, max_m, max_n, s);
+}

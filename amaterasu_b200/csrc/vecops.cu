@@ -191,3 +191,107 @@ extern "C" int ama_lda_pz(const double* rho, int64_t npoints, double* eps, doubl
   AMA_CHECK_LAUNCH();
   return AMA_OK;
 }
+
+// ------------------------------------------------------------ per-k ragged variants
+namespace {
+
+template <typename T>
+__global__ void __launch_bounds__(kRowThreads)
+kbatch_residual_kernel(int nb, const int* __restrict__ npw, const int64_t* __restrict__ pw_off,
+                       const cx_t<T>* __restrict__ x, const cx_t<T>* __restrict__ hx, const double* __restrict__ eps,
+                       const double* __restrict__ kin, double* __restrict__ norms, const int* __restrict__ rows,
+                       int nrows, cx_t<T>* __restrict__ out) {
+  using C = cx_t<T>;
+  __shared__ double sh[32];
+  const int k = blockIdx.x / nb, n = blockIdx.x % nb;
+  const int np = npw[k];
+  const int64_t po = pw_off[k];
+  const C* xr = x + po * nb + (int64_t)n * np;
+  const C* hr = hx + po * nb + (int64_t)n * np;
+  const double* kk = kin + po;
+  const double e = eps[blockIdx.x];
+  double rr = 0.0, tk = 0.0;
+  for (int g = threadIdx.x; g < np; g += kRowThreads) {
+    const C xv = xr[g], hv = hr[g];
+    const double re = (double)hv.x - e * (double)xv.x, im = (double)hv.y - e * (double)xv.y;
+    rr += re * re + im * im;
+    tk += ((double)xv.x * xv.x + (double)xv.y * xv.y) * kk[g];
+  }
+  rr = block_sum<kRowThreads>(rr, sh);
+  tk = block_sum<kRowThreads>(tk, sh);
+  if (threadIdx.x == 0) norms[blockIdx.x] = sqrt(rr);
+  const int row = rows ? rows[blockIdx.x] : -1;
+  if (row < 0) return;
+  const double ref = fmax(tk, 1e-8);
+  C* orow = out + po * nrows + (int64_t)row * np;
+  double cc = 0.0;
+  for (int g = threadIdx.x; g < np; g += kRowThreads) {
+    const C xv = xr[g], hv = hr[g];
+    const double re = (double)hv.x - e * (double)xv.x, im = (double)hv.y - e * (double)xv.y;
+    const double q = kk[g] / ref;
+    const double poly = 27.0 + q * (18.0 + q * (12.0 + 8.0 * q));
+    const double kf = poly / (poly + 16.0 * q * q * q * q);
+    cc += kf * kf * (re * re + im * im);
+    orow[g] = mk<C>(kf * re, kf * im);
+  }
+  cc = block_sum<kRowThreads>(cc, sh);
+  const double inv = 1.0 / fmax(sqrt(cc), 1e-300);
+  for (int g = threadIdx.x; g < np; g += kRowThreads) {
+    C v = orow[g];
+    orow[g] = mk<C>((double)v.x * inv, (double)v.y * inv);
+  }
+}
+
+template <typename C>
+__global__ void kbatch_copy_kernel(int nrows, const int* __restrict__ npw, const int64_t* __restrict__ pw_off,
+                                   const C* __restrict__ src, int64_t src_rows_per_k, int64_t src_row0,
+                                   C* __restrict__ dst, int64_t dst_rows_per_k, int64_t dst_row0) {
+  const int k = blockIdx.y;
+  const int np = npw[k];
+  const int64_t po = pw_off[k];
+  const C* s = src + src_rows_per_k * po + src_row0 * np;
+  C* d = dst + dst_rows_per_k * po + dst_row0 * np;
+  const int64_t total = (int64_t)nrows * np;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x)
+    d[e] = s[e];
+}
+
+}  // namespace
+
+extern "C" int ama_kbatch_residual(int32_t precision, int32_t nk, int32_t nbands, const int32_t* npw,
+                                   const int64_t* pw_off, const void* x, const void* hx, const double* eps,
+                                   const double* kinetic, double* norms, const int32_t* rows, int32_t nrows,
+                                   void* out, void* stream) {
+  AMA_REQUIRE(precision == AMA_C64 || precision == AMA_C128, AMA_ERR_ARG, "bad precision");
+  AMA_REQUIRE(npw && pw_off && x && hx && eps && kinetic && norms, AMA_ERR_ARG, "null argument");
+  AMA_REQUIRE(nk >= 1 && nbands >= 1, AMA_ERR_SHAPE, "bad sizes");
+  AMA_REQUIRE(!rows || (out && nrows >= 1), AMA_ERR_ARG, "out required with rows");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (precision == AMA_C64)
+    kbatch_residual_kernel<float><<<nk * nbands, kRowThreads, 0, s>>>(
+        nbands, npw, pw_off, (const float2*)x, (const float2*)hx, eps, kinetic, norms, rows, nrows, (float2*)out);
+  else
+    kbatch_residual_kernel<double><<<nk * nbands, kRowThreads, 0, s>>>(
+        nbands, npw, pw_off, (const double2*)x, (const double2*)hx, eps, kinetic, norms, rows, nrows, (double2*)out);
+  AMA_CHECK_LAUNCH();
+  return AMA_OK;
+}
+
+extern "C" int ama_kbatch_copy_rows(int32_t precision, int32_t nk, int32_t nrows, const int32_t* npw,
+                                    const int64_t* pw_off, const void* src, int64_t src_rows_per_k,
+                                    int64_t src_row0, void* dst, int64_t dst_rows_per_k, int64_t dst_row0,
+                                    void* stream) {
+  AMA_REQUIRE(precision == AMA_C64 || precision == AMA_C128, AMA_ERR_ARG, "bad precision");
+  AMA_REQUIRE(npw && pw_off && src && dst, AMA_ERR_ARG, "null argument");
+  if (nrows <= 0) return AMA_OK;
+  dim3 grid(32, nk);
+  cudaStream_t s = (cudaStream_t)stream;
+  if (precision == AMA_C64)
+    kbatch_copy_kernel<float2><<<grid, 256, 0, s>>>(nrows, npw, pw_off, (const float2*)src, src_rows_per_k, src_row0,
+                                                    (float2*)dst, dst_rows_per_k, dst_row0);
+  else
+    kbatch_copy_kernel<double2><<<grid, 256, 0, s>>>(nrows, npw, pw_off, (const double2*)src, src_rows_per_k,
+                                                     src_row0, (double2*)dst, dst_rows_per_k, dst_row0);
+  AMA_CHECK_LAUNCH();
+  return AMA_OK;
+}

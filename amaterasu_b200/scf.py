@@ -21,6 +21,7 @@ from dataclasses import dataclass, field
 import numpy as np
 import torch
 
+from .batched import BatchedDavidson
 from .config import Config, parse_energy
 from .density import accumulate_packed, band_weights, finalize_density
 from .eigen import davidson, random_bands
@@ -198,6 +199,17 @@ def run_scf(system, config: Config | None = None, *, logger=None, wavefunctions=
         maxit = 40 if iteration == 1 else 20
         eigenvalues = np.empty((system.nspin, system.nkpoints, nb))
         for spin in range(system.nspin):
+            if config.engine.batched:
+                # every k-point in lockstep: one launch per step over all k
+                key = ("_batched_davidson", orb.dtype)
+                bd = getattr(system, "_bd_cache", {}).get(key)
+                if bd is None:
+                    bd = BatchedDavidson(system, nb, orb.dtype)
+                    system._bd_cache = {**getattr(system, "_bd_cache", {}), key: bd}
+                eps, X, _, _ = bd.run(H, orb.packed[spin], tolerance=tol, max_iterations=maxit, spin=spin)
+                eigenvalues[spin] = eps
+                orb.packed[spin].copy_(X)
+                continue
             for ik, sphere in enumerate(system.wave_spheres):
                 res = davidson(lambda b, ik=ik, spin=spin: H.apply(b, ik, spin), orb.block(spin, ik),
                                kin_dev[ik], tolerance=tol, max_iterations=maxit)

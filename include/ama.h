@@ -114,6 +114,28 @@ AMA_API int ama_zgemm(int32_t precision, int32_t trans_b, int32_t m, int32_t n, 
               const void* b, int64_t ldb, int64_t stride_b, const double* beta, void* c,
               int64_t ldc, int64_t stride_c, int32_t batch, void* stream);
 
+/* A block of rows inside per-k-point packed storage (for the batched Davidson).
+ * ragged = 1: block k starts at rows_per_k * pw_off[k] elements, rows have npw_k elements,
+ *             and the operand starts at row row0 of the block;
+ * ragged = 0: block k starts at k * kstride elements, rows have ld elements, row row0. */
+typedef struct AmaKOperand {
+  void* base;
+  int64_t rows_per_k;
+  int64_t row0;
+  int32_t ragged;
+  int64_t ld;
+  int64_t kstride;
+} AmaKOperand;
+
+/* One complex GEMM per k-point in a single launch (forms as ama_zgemm: 0 NN, 1 NC, 2 CN);
+ * m, n or k equal to -1 mean the k-point's plane-wave count npw[k] (device int32 [nk]);
+ * pw_off (device int64 [nk]) are the prefix sums of npw; max_m/max_n bound the shapes.
+ * Replaces the per-k ndarray products of davidson/rayleigh_ritz run over every k. */
+AMA_API int ama_kbatch_zgemm(int32_t precision, int32_t form, int32_t nk, int32_t m, int32_t n, int32_t k,
+                             const int32_t* npw, const int64_t* pw_off, const AmaKOperand* a,
+                             const AmaKOperand* b, const AmaKOperand* c, const double* alpha,
+                             const double* beta, int32_t max_m, int32_t max_n, void* stream);
+
 /* Teter-Payne-Allan preconditioning fused with the residual and normalisation:
  *   r = hx - eps*x; t_n = sum_G |x|^2 T_G; out = K(T_G / max(t_n,1e-8)) r / ||.||
  * for the `nrows` rows listed in `rows` (device int32); norms (device FP64 [nbands]) get
@@ -150,6 +172,21 @@ AMA_API int ama_grid_filter_noalloc(AmaEngine* engine, int32_t slot, int32_t ene
  * [n1*n2*n3], device complex128 out [n1*n2*n3]): out[G] = (1/N) sum_r in(r) e^{-iG.r}.
  * Replaces FFTGrid.to_reciprocal on a density (basis/fft.py:228-235). */
 AMA_API int ama_grid_fft_forward(AmaEngine* engine, const double* in, void* out, void* stream);
+
+/* ama_residual_precondition for every k-point in one launch: x/hx packed (nbands, npw_k)
+ * blocks, eps/norms [nk][nbands], kinetic packed by pw_off; rows [nk][nbands] gives the
+ * output row of each band's correction (-1: none) in out, packed (nrows, npw_k) blocks. */
+AMA_API int ama_kbatch_residual(int32_t precision, int32_t nk, int32_t nbands, const int32_t* npw,
+                                const int64_t* pw_off, const void* x, const void* hx, const double* eps,
+                                const double* kinetic, double* norms, const int32_t* rows, int32_t nrows,
+                                void* out, void* stream);
+
+/* Copy nrows rows per k-point between packed per-k blocks (block k at rows_per_k*pw_off[k],
+ * rows of npw_k elements, starting at row row0). */
+AMA_API int ama_kbatch_copy_rows(int32_t precision, int32_t nk, int32_t nrows, const int32_t* npw,
+                                 const int64_t* pw_off, const void* src, int64_t src_rows_per_k,
+                                 int64_t src_row0, void* dst, int64_t dst_rows_per_k, int64_t dst_row0,
+                                 void* stream);
 
 /* LDA exchange plus Perdew-Zunger 1981 correlation on a spin-resolved density
  * (device FP64, rho [2][npoints]); writes eps_xc [npoints] and v_xc [2][npoints].

@@ -108,3 +108,24 @@ def test_batched_jacobi_matches_eigh(n):
         np.testing.assert_allclose(w[b], ref, rtol=0, atol=1e-11 * max(1.0, np.abs(ref).max()))
         np.testing.assert_allclose(v[b].conj().T @ v[b], np.eye(n), atol=1e-12)
         np.testing.assert_allclose(a[b] @ v[b], v[b] * w[b][None, :], atol=1e-10 * max(1.0, np.abs(ref).max()))
+
+
+@pytest.mark.parametrize("dtype,tol", [(torch.complex128, 1e-9), (torch.complex64, 1e-5)])
+def test_batched_davidson_matches_per_k(mini_system, dtype, tol):
+    """All k-points in lockstep (batched launches) against the reference's per-k result."""
+    from amaterasu_b200.batched import BatchedDavidson
+    from amaterasu_b200.hamiltonian import Hamiltonian
+    g = golden("mini.npz")
+    s = mini_system
+    H = Hamiltonian(s, g["veff"], precision="complex128" if dtype == torch.complex128 else "complex64")
+    guess = torch.from_numpy(np.concatenate([g["guess0"].ravel(), g["guess1"].ravel()])).cuda().to(dtype)
+    bd = BatchedDavidson(s, s.nbands, dtype)
+    eps, X, norms, it = bd.run(H, guess, tolerance=tol, max_iterations=60)
+    for ik in range(2):
+        np.testing.assert_allclose(eps[ik][:5], g[f"dav_eig{ik}"][:5], rtol=0, atol=max(tol, 1e-9) * 10)
+    # orthonormal Ritz vectors per k
+    off = 0
+    for ik, w in enumerate(s.wave_spheres):
+        blk = X[off:off + s.nbands * len(w)].reshape(s.nbands, len(w)).to(torch.complex128).cpu().numpy()
+        off += s.nbands * len(w)
+        np.testing.assert_allclose(blk @ blk.conj().T, np.eye(s.nbands), atol=1e-5 if dtype == torch.complex64 else 1e-11)

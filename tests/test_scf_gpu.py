@@ -21,9 +21,10 @@ def si2_system(si_pseudo):
     return build_system(structure, {"Si": si_pseudo}, ecut, 4 * ecut, kpoints=ks, nbands=nb)
 
 
-def _config(precision):
+def _config(precision, batched=True):
     from amaterasu_b200.config import Config
     c = Config()
+    c.engine.batched = batched
     c.occupations.scheme = "fixed"
     c.occupations.nbands = 8
     c.scf.tol_energy = 1e-8
@@ -32,13 +33,13 @@ def _config(precision):
     return c
 
 
-@pytest.mark.parametrize("precision", ["complex128", "mixed"])
-def test_si2_scf_matches_reference(si2_system, precision):
+@pytest.mark.parametrize("precision,batched", [("complex128", True), ("mixed", True), ("complex128", False)])
+def test_si2_scf_matches_reference(si2_system, precision, batched):
     from amaterasu_b200.scf import run_scf
     from amaterasu_b200.units import HARTREE_IN_EV
     g = golden("si2_scf.npz")
     s = si2_system
-    res = run_scf(s, _config(precision), logger=print)
+    res = run_scf(s, _config(precision, batched), logger=print)
     assert res.converged
     e = res.energies
     natoms = s.natoms
