@@ -11,7 +11,9 @@ three times per iteration for the whole set instead of per k.
 Storage: the basis of k-point k is a (cap, npw_k) block at cap * pw_off[k]; every k carries
 the same number of rows. When a k-point has fewer new directions than the others (fewer
 active bands, or directions dropped as dependent), its surplus rows are zero and marked
-invalid: their Rayleigh-Ritz diagonal is set far above the spectrum, which decouples them.
+invalid: their Rayleigh-Ritz diagonal is set just above that k's Gershgorin bound of the
+valid block, which decouples them without inflating the matrix norm (the Jacobi solver's
+stopping rule is relative to it).
 Orthonormalisation (initial block and new directions) uses the Gram eigendecomposition,
 which spans the same space as the reference's Cholesky/SVD, so the Ritz pairs agree.
 """
@@ -25,7 +27,7 @@ import torch
 from ._lib import AMA_C64, AMA_C128, AmaKOperand, call
 from .engine import engine_for, ptr, stream_ptr
 
-_BIG = 1.0e6          # Ha, diagonal of invalid Rayleigh-Ritz rows
+_GAP = 1.0            # Ha, invalid Rayleigh-Ritz rows sit this far above the Gershgorin bound
 _JACOBI_MAX = 80
 
 
@@ -127,7 +129,8 @@ class BatchedDavidson:
         p = 0.5 * (p + p.conj().transpose(1, 2))
         inval = torch.from_numpy(~valid[:, :m]).to(self.dev)
         p = p * (~inval)[:, :, None] * (~inval)[:, None, :]
-        p = p + torch.diag_embed(inval.to(torch.float64) * _BIG).to(torch.complex128)
+        bound = p.abs().sum(dim=2).max(dim=1, keepdim=True).values + _GAP  # per-k Gershgorin bound
+        p = p + torch.diag_embed(inval.to(torch.float64) * bound).to(torch.complex128)
         w, v = self._heev(p)
         rot = v[:, :, :self.nb].transpose(1, 2)  # (nb x m) per k: X_n = sum_i V[i, n] b_i
         X = self._rotate(rot, B, self.cap, m, self.nb)

@@ -170,39 +170,39 @@ __device__ __forceinline__ void contig_task(C* __restrict__ base, int es, int n,
 }
 
 // Column mode: consecutive threads take consecutive columns (conflict-free smem).
-template <int RA, int S, bool TW, typename C>
+template <int RA, int S, bool TW, int NT = kFftThreads, typename C>
 __device__ void strided_cols(C* sm, int n, int ncols, const C* tw) {
   const int B = n / RA;
   const int tasks = B * ncols;
-  for (int t = threadIdx.x; t < tasks; t += kFftThreads) {
+  for (int t = threadIdx.x; t < tasks; t += NT) {
     const int col = t % ncols, b = t / ncols;
     strided_task<RA, S, TW>(sm + col, ncols, n, b, tw);
   }
 }
-template <int RB, int S, bool TW, typename C>
+template <int RB, int S, bool TW, int NT = kFftThreads, typename C>
 __device__ void contig_cols(C* sm, int n, int ncols, const C* tw) {
   const int A = n / RB;
   const int tasks = A * ncols;
-  for (int t = threadIdx.x; t < tasks; t += kFftThreads) {
+  for (int t = threadIdx.x; t < tasks; t += NT) {
     const int col = t % ncols, c = t / ncols;
     contig_task<RB, S, TW>(sm + col, ncols, n, c, tw);
   }
 }
 // Row mode over a list of row indices (rows have stride `ld`).
-template <int RA, int S, bool TW, typename C>
+template <int RA, int S, bool TW, int NT = kFftThreads, typename C>
 __device__ void strided_rows(C* sm, int n, int ld, const int* rows, int nrows, const C* tw) {
   const int B = n / RA;
   const int tasks = B * nrows;
-  for (int t = threadIdx.x; t < tasks; t += kFftThreads) {
+  for (int t = threadIdx.x; t < tasks; t += NT) {
     const int b = t % B, r = rows[t / B];
     strided_task<RA, S, TW>(sm + r * ld, 1, n, b, tw);
   }
 }
-template <int RB, int S, bool TW, typename C>
+template <int RB, int S, bool TW, int NT = kFftThreads, typename C>
 __device__ void contig_rows(C* sm, int n, int ld, const int* rows, int nrows, const C* tw) {
   const int A = n / RB;
   const int tasks = A * nrows;
-  for (int t = threadIdx.x; t < tasks; t += kFftThreads) {
+  for (int t = threadIdx.x; t < tasks; t += NT) {
     const int c = t % A, r = rows[t / A];
     contig_task<RB, S, TW>(sm + r * ld, 1, n, c, tw);
   }
@@ -217,30 +217,30 @@ __device__ void contig_rows(C* sm, int n, int ld, const int* rows, int nrows, co
 // Permuted input, natural output: contiguous(B, twiddle) then strided(A). The sign S
 // only selects the codelet direction; `tw` must hold w_n^(S t). Each pass ends with a
 // block barrier.
-template <int S, bool NAT_IN = (S > 0), typename C>
+template <int S, bool NAT_IN = (S > 0), int NT = kFftThreads, typename C>
 __device__ void dft_cols(C* sm, int n, int A, int B, int ncols, const C* tw) {
   if constexpr (NAT_IN) {
     switch (A) {
-#define CASE(R) case R: strided_cols<R, S, true>(sm, n, ncols, tw); break;
+#define CASE(R) case R: strided_cols<R, S, true, NT>(sm, n, ncols, tw); break;
       AMA_RADIX_CASES(CASE)
 #undef CASE
     }
     __syncthreads();
     switch (B) {
-#define CASE(R) case R: contig_cols<R, S, false>(sm, n, ncols, tw); break;
+#define CASE(R) case R: contig_cols<R, S, false, NT>(sm, n, ncols, tw); break;
       AMA_RADIX_CASES(CASE)
 #undef CASE
     }
     __syncthreads();
   } else {
     switch (B) {
-#define CASE(R) case R: contig_cols<R, S, true>(sm, n, ncols, tw); break;
+#define CASE(R) case R: contig_cols<R, S, true, NT>(sm, n, ncols, tw); break;
       AMA_RADIX_CASES(CASE)
 #undef CASE
     }
     __syncthreads();
     switch (A) {
-#define CASE(R) case R: strided_cols<R, S, false>(sm, n, ncols, tw); break;
+#define CASE(R) case R: strided_cols<R, S, false, NT>(sm, n, ncols, tw); break;
       AMA_RADIX_CASES(CASE)
 #undef CASE
     }
@@ -248,31 +248,31 @@ __device__ void dft_cols(C* sm, int n, int A, int B, int ncols, const C* tw) {
   }
 }
 
-template <int S, bool NAT_IN = (S > 0), typename C>
+template <int S, bool NAT_IN = (S > 0), int NT = kFftThreads, typename C>
 __device__ void dft_rows(C* sm, int n, int A, int B, int ld, const int* rows, int nrows,
                          const C* tw) {
   if constexpr (NAT_IN) {
     switch (A) {
-#define CASE(R) case R: strided_rows<R, S, true>(sm, n, ld, rows, nrows, tw); break;
+#define CASE(R) case R: strided_rows<R, S, true, NT>(sm, n, ld, rows, nrows, tw); break;
       AMA_RADIX_CASES(CASE)
 #undef CASE
     }
     __syncthreads();
     switch (B) {
-#define CASE(R) case R: contig_rows<R, S, false>(sm, n, ld, rows, nrows, tw); break;
+#define CASE(R) case R: contig_rows<R, S, false, NT>(sm, n, ld, rows, nrows, tw); break;
       AMA_RADIX_CASES(CASE)
 #undef CASE
     }
     __syncthreads();
   } else {
     switch (B) {
-#define CASE(R) case R: contig_rows<R, S, true>(sm, n, ld, rows, nrows, tw); break;
+#define CASE(R) case R: contig_rows<R, S, true, NT>(sm, n, ld, rows, nrows, tw); break;
       AMA_RADIX_CASES(CASE)
 #undef CASE
     }
     __syncthreads();
     switch (A) {
-#define CASE(R) case R: strided_rows<R, S, false>(sm, n, ld, rows, nrows, tw); break;
+#define CASE(R) case R: strided_rows<R, S, false, NT>(sm, n, ld, rows, nrows, tw); break;
       AMA_RADIX_CASES(CASE)
 #undef CASE
     }

@@ -370,7 +370,9 @@ StageInfo fill_stage_table(const void** fn) {
 }
 
 // complex64 on a compile-time grid with short x columns: register-resident stage B
-template <int N1, int A1, class D>
+// (register-resident y columns for stages A and C were measured slower than the
+// shared-memory passes at 84^3 and are not used)
+template <int N1, int A1, int N2, int A2, int N3, class D>
 StageInfo fill_stage_table_reg(const void** fn) {
   StageInfo info = fill_stage_table<float, D>(fn);
   fn[1] = (const void*)stage_b_reg_kernel<N1, A1, D>;
@@ -387,7 +389,7 @@ StageInfo select_stage_table(const AxisPlan* ax, const void** fn) {
       ax[2].A == A3) {                                                                           \
     using D = FixDims<N1, A1, N2, A2, N3, A3>;                                                   \
     if constexpr (std::is_same<T, float>::value && N1 <= 96)                                     \
-      return fill_stage_table_reg<N1, A1, D>(fn);                                                \
+      return fill_stage_table_reg<N1, A1, N2, A2, N3, D>(fn);                                    \
     else                                                                                         \
       return fill_stage_table<T, D>(fn);                                                         \
   }

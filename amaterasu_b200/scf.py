@@ -102,6 +102,7 @@ class _Orbitals:
 
 
 def _kinetic_energy(system, orb: _Orbitals, occ, kin_dev) -> float:
+    """Local (this rank's k-points) kinetic energy; occ holds this rank's k-points."""
     g = 2.0 / system.nspin
     total = torch.zeros((), dtype=torch.float64, device=orb.packed[0].device)
     for spin in range(system.nspin):
@@ -128,15 +129,26 @@ def _nonlocal_energy(system, orb: _Orbitals, occ, dij_dev) -> float:
     return float(total)
 
 
-def _density_out(system, orb: _Orbitals, occ) -> torch.Tensor:
+def _density_out(system, orb: _Orbitals, occ, comm=None) -> torch.Tensor:
     rho = torch.zeros((system.nspin, orb.eng.N), dtype=torch.float64, device=orb.packed[0].device)
     for spin in range(system.nspin):
         accumulate_packed(system, orb.packed[spin], orb.nbands, band_weights(system, occ, spin), rho[spin])
+    if comm is not None:
+        comm.allreduce_(rho)  # partial densities of the ranks' k-points
     return finalize_density(system, rho)
 
 
-def run_scf(system, config: Config | None = None, *, logger=None, wavefunctions=None, density=None) -> SCFResult:
-    """Run the SCF loop to self-consistency on the GPU."""
+def run_scf(system, config: Config | None = None, *, logger=None, wavefunctions=None, density=None,
+            comm=None) -> SCFResult:
+    """Run the SCF loop to self-consistency on the GPU.
+
+    With ``comm`` (a :class:`~amaterasu_b200.parallel.KpointComm` of several ranks) the
+    system must be this rank's shard (:func:`~amaterasu_b200.parallel.shard_system`): the
+    rank solves its own k-points and the density, eigenvalues and band energies are
+    combined across ranks every iteration."""
+    distributed = comm is not None and comm.world > 1
+    if distributed and not hasattr(system, "kparts"):
+        raise ValueError("a distributed SCF needs the rank's shard of the system (parallel.shard_system)")
     config = config or Config()
     if config.scf.method != "mixing":
         raise NotImplementedError(f"scf.method {config.scf.method!r}: only density mixing is implemented")
@@ -215,23 +227,37 @@ def run_scf(system, config: Config | None = None, *, logger=None, wavefunctions=
                                kin_dev[ik], tolerance=tol, max_iterations=maxit)
                 eigenvalues[spin, ik] = res.eigenvalues.cpu().numpy()
                 orb.set(spin, ik, res.coefficients)
-        occ_result = compute_occupations(eigenvalues, system.kpoints.weights, system.nelectrons,
+        if distributed:
+            eig_all = comm.gather_eigenvalues(eigenvalues, system.kparts)
+            weights_all = system.global_weights
+        else:
+            eig_all, weights_all = eigenvalues, system.kpoints.weights
+        occ_result = compute_occupations(eig_all, weights_all, system.nelectrons,
                                          scheme=config.occupations.scheme, smearing=smearing,
                                          order=config.occupations.order, nspin=system.nspin)
-        occ = occ_result.occupations
-        rho_out = _density_out(system, orb, occ)
+        occ_all = occ_result.occupations
+        if distributed:
+            k0, kc = system.kparts[system.krank]
+            occ = occ_all[:, k0:k0 + kc]
+        else:
+            occ = occ_all
+        rho_out = _density_out(system, orb, occ, comm if distributed else None)
         e_h, _ = ops.hartree(rho_out.sum(0))
         xc_d = rho_out
         if system.core_density is not None:
             xc_d = rho_out + torch.from_numpy(system.core_density.ravel()).to(dev)[None] / system.nspin
         e_xc, _ = ops.lda(xc_d)
+        e_kin = _kinetic_energy(system, orb, occ, kin_dev)
+        e_nl = _nonlocal_energy(system, orb, occ, dij_dev)
+        if distributed:
+            e_kin, e_nl = comm.allreduce_scalars([e_kin, e_nl])
         energies = Energies(
-            kinetic=_kinetic_energy(system, orb, occ, kin_dev),
+            kinetic=float(e_kin),
             local=float((vloc * rho_out.sum(0)).sum()) * dv,
             hartree=float(e_h), xc=float(e_xc),
-            nonlocal_=_nonlocal_energy(system, orb, occ, dij_dev),
+            nonlocal_=float(e_nl),
             ewald=system.ewald, entropy=occ_result.entropy_term)
-        band_sum = 2.0 / system.nspin * float(np.einsum("k,skn,skn->", system.kpoints.weights, occ, eigenvalues))
+        band_sum = 2.0 / system.nspin * float(np.einsum("k,skn,skn->", weights_all, occ_all, eig_all))
         local_e = float((veff.reshape(system.nspin, -1) * rho_out).sum()) * dv
         identity = band_sum - (energies.kinetic + local_e + energies.nonlocal_)
         residual = float((rho_out - rho_in).abs().sum()) * dv / system.nelectrons
@@ -251,8 +277,8 @@ def run_scf(system, config: Config | None = None, *, logger=None, wavefunctions=
     wfs = [[orb.block(spin, ik).clone() for ik in range(system.nkpoints)] for spin in range(system.nspin)]
     dens = rho_out.reshape(system.nspin, *system.grid.shape).cpu().numpy()
     return SCFResult(
-        converged=converged, iterations=iteration, energies=energies, eigenvalues=eigenvalues,
-        occupations=occ_result.occupations, fermi_level=occ_result.fermi_level, gap=occ_result.gap,
+        converged=converged, iterations=iteration, energies=energies, eigenvalues=eig_all,
+        occupations=occ_all, fermi_level=occ_result.fermi_level, gap=occ_result.gap,
         magnetization=occ_result.magnetization, density=dens, wavefunctions=wfs, history=history,
         electron_count=float(dens.sum()) * dv, seconds=time.perf_counter() - started,
         precision_trace=trace, seconds_per_iteration=step_times)
