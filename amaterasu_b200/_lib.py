@@ -66,6 +66,8 @@ SIGNATURES = {
     "ama_lda_pz": (ct.c_int, [_P, _I64, _P, _P, _P]),
     "ama_kbatch_zgemm": (ct.c_int, [_I32, _I32, _I32, _I32, _I32, _I32, _P, _P, _P, _P, _P, _P, _P, _I32, _I32,
                                     _P]),
+    "ama_kbatch_zgemm_tc": (ct.c_int, [_I32, _I32, _I32, _I32, _I32, _P, _P, _P, _P, _P, _P, _P, _I32, _P]),
+    "ama_subspace_tc_status": (ct.c_int, [ct.POINTER(ct.c_int32)]),
     "ama_kbatch_residual": (ct.c_int, [_I32, _I32, _I32, _P, _P, _P, _P, _P, _P, _P, _P, _I32, _P, _P]),
     "ama_kbatch_copy_rows": (ct.c_int, [_I32, _I32, _I32, _P, _P, _P, _I64, _I64, _P, _I64, _I64, _P]),
     "ama_set_grid_filter": (ct.c_int, [_P, _I32, _P]),

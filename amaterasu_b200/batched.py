@@ -29,6 +29,7 @@ from .engine import engine_for, ptr, stream_ptr
 
 _GAP = 1.0            # Ha, invalid Rayleigh-Ritz rows sit this far above the Gershgorin bound
 _JACOBI_MAX = 80
+_TC_MIN_NPW = 8192
 
 
 class _KOp:
@@ -41,7 +42,7 @@ class _KOp:
 
 
 class BatchedDavidson:
-    def __init__(self, system, nbands: int, dtype=torch.complex128):
+    def __init__(self, system, nbands: int, dtype=torch.complex128, tensor_cores: bool = True):
         self.eng = engine_for(system)
         self.system = system
         self.nk = self.eng.nk
@@ -57,11 +58,18 @@ class BatchedDavidson:
         self.kin = torch.from_numpy(np.concatenate([s.kinetic_energy for s in system.wave_spheres])).to(dev)
         self.max_sub = min(4 * nbands, int(self.eng.npw.min()))
         self.cap = self.max_sub + nbands
+        # complex64 plane-wave products on the tensor cores (split-TF32) once the spheres are
+        # long enough for the staged tiles to pay; shorter ones stay on the SIMT kernels
+        self.tensor_cores = bool(tensor_cores) and dtype == torch.complex64 and self.max_npw >= _TC_MIN_NPW
 
     # ---------------------------------------------------------------- kernels
     def _gemm(self, form, m, n, k, a: _KOp, b: _KOp, c: _KOp, alpha=1.0, beta=0.0, max_m=None, max_n=None):
         al = (ct.c_double * 2)(float(np.real(alpha)), float(np.imag(alpha)))
         be = (ct.c_double * 2)(float(np.real(beta)), float(np.imag(beta)))
+        if self.tensor_cores and ((form == 1 and k < 0 and m > 0 and n > 0) or (form == 0 and n < 0 and m > 0 and k > 0)):
+            call("ama_kbatch_zgemm_tc", form, self.nk, m, n, k, ptr(self.npw), ptr(self.pw_off),
+                 ct.byref(a.c), ct.byref(b.c), ct.byref(c.c), al, be, self.max_npw, stream_ptr())
+            return
         mm = max_m if max_m is not None else (self.max_npw if m < 0 else m)
         nn = max_n if max_n is not None else (self.max_npw if n < 0 else n)
         call("ama_kbatch_zgemm", self.prec, form, self.nk, m, n, k, ptr(self.npw), ptr(self.pw_off),

@@ -57,10 +57,15 @@ class EngineConfig:
     """Engine-only options.
 
     ``precision``: "complex128" (plain FP64), "complex64", or "mixed" (complex64 bulk,
-    complex128 once the density residual drops below ``refine_below``).
+    complex128 once the density residual drops below ``refine_below``, or once the best
+    residual of the last ``stall_window`` complex64 iterations is not below ``stall_ratio``
+    times the best one before them).
     """
     precision: str = "complex128"
     refine_below: float = 1e-6
+    stall_window: int = 3
+    stall_ratio: float = 0.7
+    tc_subspace: bool = True  # complex64 Davidson plane-wave products on the tensor cores
     batched: bool = True
 
 

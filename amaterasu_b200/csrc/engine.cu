@@ -594,11 +594,11 @@ int hpsi_impl(AmaEngine* e, int k_first, int k_count, int nbands, int spin, cons
     splits = std::min(splits, std::max(1, maxnpw / 256));
     const int64_t pstride = (int64_t)nbands * e->nproj;
     if (splits > 1)
-      AMA_CUDA_TRY(grow<char>(&e->ws_part[p], &e->ws_part_bytes[p], (size_t)k_count * splits * pstride * el));
+      AMA_CUDA_TRY(grow<char>(&e->ws_part[p], &e->ws_part_bytes[p], (size_t)k_count * splits * pstride * sizeof(double2)));
     ProjectBatch<C> pb{(const C*)psi, (const C*)e->d.proj[p], (C*)e->ws_proj[p], e->d.pw_off, e->d.npw,
                        k_first, nbands, e->nproj};
     AMA_CUDA_TRY((launch_cgemm<T, kNC>(pb, k_count, nbands, e->nproj, splits, mk<C>(1, 0), mk<C>(0, 0),
-                                       (C*)e->ws_part[p], pstride, s)));
+                                       (double2*)e->ws_part[p], pstride, s)));
     ApplyBatch<C> ab{(const C*)e->ws_proj[p], (const C*)e->d.dproj[p], (C*)hpsi, e->d.pw_off, e->d.npw,
                      k_first, nbands, e->nproj};
     AMA_CUDA_TRY((launch_cgemm<T, kNN>(ab, k_count, nbands, maxnpw, 1, mk<C>(1, 0), mk<C>(1, 0),
@@ -911,10 +911,10 @@ static int project_impl(AmaEngine* e, int k, int nbands, const void* psi, void* 
   splits = std::min(splits, std::max(1, e->npw[k] / 256));
   const int64_t pstride = (int64_t)nbands * e->nproj;
   if (splits > 1)
-    AMA_CUDA_TRY(grow<char>(&e->ws_part[p], &e->ws_part_bytes[p], (size_t)splits * pstride * sizeof(C)));
+    AMA_CUDA_TRY(grow<char>(&e->ws_part[p], &e->ws_part_bytes[p], (size_t)splits * pstride * sizeof(double2)));
   ProjectBatch<C> pb{(const C*)psi, (const C*)e->d.proj[p], (C*)out, e->d.pw_off, e->d.npw, k, nbands, e->nproj};
   AMA_CUDA_TRY((launch_cgemm<T, kNC>(pb, 1, nbands, e->nproj, splits, mk<C>(1, 0), mk<C>(0, 0),
-                                     (C*)e->ws_part[p], pstride, s)));
+                                     (double2*)e->ws_part[p], pstride, s)));
   return AMA_OK;
 }
 

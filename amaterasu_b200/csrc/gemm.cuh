@@ -1,5 +1,8 @@
 // Complex GEMM on the SIMT pipes (FP32 or FP64), tiled 64x64 per CTA with a 4x4
 // complex micro-tile per thread, split-K over a partial-sum buffer for long reductions.
+// The FP32 form adds its running sums into FP64 registers every kFlushTiles k-tiles
+// (128 products), so a long reduction (plane-wave count ~1e5) carries the rounding of a
+// 128-term FP32 sum, not of the whole sum; split-K partials are FP64 for both precisions.
 //
 // Forms (all row-major):
 //   NN : C = alpha * A(m x k) * B(k x n)        + beta * C
@@ -9,6 +12,8 @@
 // which lets the engine run ragged per-k products (different npw per k) in one launch.
 #pragma once
 #include "common.cuh"
+
+#include <type_traits>
 
 namespace ama {
 
@@ -23,13 +28,14 @@ template <typename C> struct GemmProblem {
 constexpr int kBM = 64, kBN = 64, kGemmThreads = 256;
 template <typename T> struct GemmBK { static constexpr int value = 16; };
 template <> struct GemmBK<double> { static constexpr int value = 8; };
+constexpr int kFlushTiles = 8;  // FP32: 8 k-tiles of 16 = 128 products per FP32 partial sum
 
 // One CTA computes a kBM x kBN tile of batch blockIdx.z / splits, reduction slice
 // blockIdx.z % splits. If `partial` is non-null the raw tile sum goes to
 // partial[(z_split * M*N ...)] (see engine), else the alpha/beta epilogue is applied.
 template <typename T, int FORM, class Batch>
 __global__ void __launch_bounds__(kGemmThreads)
-cgemm_tile_kernel(Batch batch, int splits, cx_t<T> alpha, cx_t<T> beta, cx_t<T>* partial,
+cgemm_tile_kernel(Batch batch, int splits, cx_t<T> alpha, cx_t<T> beta, double2* partial,
                   int64_t partial_stride) {
   using C = cx_t<T>;
   constexpr int BK = GemmBK<T>::value;
@@ -47,12 +53,21 @@ cgemm_tile_kernel(Batch batch, int splits, cx_t<T> alpha, cx_t<T> beta, cx_t<T>*
 
   const int tid = threadIdx.x;
   const int tx = tid % 16, ty = tid / 16;
+  constexpr bool kFlush = std::is_same<T, float>::value;
   C acc[4][4];
+  double2 dacc[kFlush ? 4 : 1][kFlush ? 4 : 1];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j] = mk<C>(0, 0);
+  if constexpr (kFlush) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) dacc[i][j] = make_double2(0.0, 0.0);
+  }
 
+  int tile_count = 0;
   for (int k0 = kbeg; k0 < kend; k0 += BK) {
     // ---- A tile -> As[kk][mm]
     for (int e = tid; e < BK * kBM; e += kGemmThreads) {
@@ -97,7 +112,31 @@ cgemm_tile_kernel(Batch batch, int splits, cx_t<T> alpha, cx_t<T> beta, cx_t<T>*
         }
     }
     __syncthreads();
+    if constexpr (kFlush) {
+      if (++tile_count == kFlushTiles) {
+        tile_count = 0;
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            dacc[i][j].x += (double)acc[i][j].x;
+            dacc[i][j].y += (double)acc[i][j].y;
+            acc[i][j] = mk<C>(0, 0);
+          }
+      }
+    }
   }
+  // the tile's sums in FP64
+  double2 sum[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      if constexpr (kFlush)
+        sum[i][j] = make_double2(dacc[i][j].x + (double)acc[i][j].x, dacc[i][j].y + (double)acc[i][j].y);
+      else
+        sum[i][j] = make_double2((double)acc[i][j].x, (double)acc[i][j].y);
+    }
 
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
@@ -108,10 +147,10 @@ cgemm_tile_kernel(Batch batch, int splits, cx_t<T> alpha, cx_t<T> beta, cx_t<T>*
       const int gn = n0 + tx + 16 * j;
       if (gn >= p.n) continue;
       if (partial) {
-        partial[(int64_t)z * partial_stride + (int64_t)gm * p.n + gn] = acc[i][j];
+        partial[(int64_t)z * partial_stride + (int64_t)gm * p.n + gn] = sum[i][j];
       } else {
         C* dst = p.c + (int64_t)gm * p.ldc + gn;
-        C r = cmul(alpha, acc[i][j]);
+        C r = cmul(alpha, mk<C>(sum[i][j].x, sum[i][j].y));
         if (beta.x != T(0) || beta.y != T(0)) r = cadd(r, cmul(beta, *dst));
         *dst = r;
       }
@@ -122,29 +161,33 @@ cgemm_tile_kernel(Batch batch, int splits, cx_t<T> alpha, cx_t<T> beta, cx_t<T>*
 // Sum the split-K partials of each batch and apply the epilogue.
 template <typename T, class Batch>
 __global__ void cgemm_reduce_kernel(Batch batch, int splits, cx_t<T> alpha, cx_t<T> beta,
-                                    const cx_t<T>* partial, int64_t partial_stride) {
+                                    const double2* partial, int64_t partial_stride) {
   using C = cx_t<T>;
   const int bz = blockIdx.y;
   const GemmProblem<C> p = batch(bz);
   const int64_t total = (int64_t)p.m * p.n;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
        e += (int64_t)gridDim.x * blockDim.x) {
-    C s = mk<C>(0, 0);
-    for (int sidx = 0; sidx < splits; ++sidx)
-      s = cadd(s, partial[(int64_t)(bz * splits + sidx) * partial_stride + e]);
+    double2 s = make_double2(0.0, 0.0);
+    for (int sidx = 0; sidx < splits; ++sidx) {
+      const double2 v = partial[(int64_t)(bz * splits + sidx) * partial_stride + e];
+      s.x += v.x;
+      s.y += v.y;
+    }
     const int gm = (int)(e / p.n), gn = (int)(e % p.n);
     C* dst = p.c + (int64_t)gm * p.ldc + gn;
-    C r = cmul(alpha, s);
+    C r = cmul(alpha, mk<C>(s.x, s.y));
     if (beta.x != T(0) || beta.y != T(0)) r = cadd(r, cmul(beta, *dst));
     *dst = r;
   }
 }
 
 // Launch helper. `max_m/max_n/max_k` bound the batch's sizes (grid shape); `splits` > 1
-// needs `partial` sized batch*splits*partial_stride elements with partial_stride >= m*n.
+// needs `partial` sized batch*splits*partial_stride FP64 complex elements with
+// partial_stride >= m*n.
 template <typename T, int FORM, class Batch>
 cudaError_t launch_cgemm(Batch batch, int nbatch, int max_m, int max_n, int splits,
-                         cx_t<T> alpha, cx_t<T> beta, cx_t<T>* partial, int64_t partial_stride,
+                         cx_t<T> alpha, cx_t<T> beta, double2* partial, int64_t partial_stride,
                          cudaStream_t stream) {
   dim3 grid((max_n + kBN - 1) / kBN, (max_m + kBM - 1) / kBM, nbatch * splits);
   if (splits <= 1) {

@@ -35,7 +35,7 @@ int zgemm_impl(int form, int m, int n, int k, const double* alpha, const void* a
   splits = std::min(splits, std::max(1, k / 512));
   const int64_t pstride = (int64_t)m * n;
   if (splits > 1) {
-    const size_t need = (size_t)batch * splits * pstride * sizeof(C);
+    const size_t need = (size_t)batch * splits * pstride * sizeof(double2);
     if (g_partial.bytes < need) {
       if (g_partial.ptr) cudaFree(g_partial.ptr);
       g_partial.ptr = nullptr; g_partial.bytes = 0;
@@ -44,9 +44,9 @@ int zgemm_impl(int form, int m, int n, int k, const double* alpha, const void* a
     }
   }
   cudaError_t err;
-  if (form == 0) err = launch_cgemm<T, kNN>(sbch, batch, m, n, splits, al, be, (C*)g_partial.ptr, pstride, s);
-  else if (form == 1) err = launch_cgemm<T, kNC>(sbch, batch, m, n, splits, al, be, (C*)g_partial.ptr, pstride, s);
-  else err = launch_cgemm<T, kCN>(sbch, batch, m, n, splits, al, be, (C*)g_partial.ptr, pstride, s);
+  if (form == 0) err = launch_cgemm<T, kNN>(sbch, batch, m, n, splits, al, be, (double2*)g_partial.ptr, pstride, s);
+  else if (form == 1) err = launch_cgemm<T, kNC>(sbch, batch, m, n, splits, al, be, (double2*)g_partial.ptr, pstride, s);
+  else err = launch_cgemm<T, kCN>(sbch, batch, m, n, splits, al, be, (double2*)g_partial.ptr, pstride, s);
   AMA_CUDA_TRY(err);
   return AMA_OK;
 }
@@ -125,10 +125,27 @@ int kbatch_impl(int form, int nk, int m, int n, int k, const int32_t* npw, const
   using C = cx_t<T>;
   KBatch<C> kb{to_kop(a), to_kop(b), to_kop(c), m, n, k, npw, pw_off};
   const C al = mk<C>(alpha[0], alpha[1]), be = mk<C>(beta[0], beta[1]);
+  // split a long (plane-wave) reduction when the tile grid alone does not fill the GPU
+  int splits = 1;
+  if (k < 0) {  // a slice shorter than one k-tile (few plane waves) just writes zeros
+    const int tiles = ((max_m + kBM - 1) / kBM) * ((max_n + kBN - 1) / kBN) * nk;
+    splits = std::max(1, std::min(32, (2 * 148 + tiles - 1) / tiles));
+  }
+  const int64_t pstride = (int64_t)max_m * max_n;
+  if (splits > 1) {
+    const size_t need = (size_t)nk * splits * pstride * sizeof(double2);
+    if (g_partial.bytes < need) {
+      if (g_partial.ptr) cudaFree(g_partial.ptr);
+      g_partial.ptr = nullptr; g_partial.bytes = 0;
+      AMA_CUDA_TRY(cudaMalloc(&g_partial.ptr, need));
+      g_partial.bytes = need;
+    }
+  }
+  double2* part = (double2*)g_partial.ptr;
   cudaError_t err;
-  if (form == 0) err = launch_cgemm<T, kNN>(kb, nk, max_m, max_n, 1, al, be, (C*)nullptr, 0, s);
-  else if (form == 1) err = launch_cgemm<T, kNC>(kb, nk, max_m, max_n, 1, al, be, (C*)nullptr, 0, s);
-  else err = launch_cgemm<T, kCN>(kb, nk, max_m, max_n, 1, al, be, (C*)nullptr, 0, s);
+  if (form == 0) err = launch_cgemm<T, kNN>(kb, nk, max_m, max_n, splits, al, be, part, pstride, s);
+  else if (form == 1) err = launch_cgemm<T, kNC>(kb, nk, max_m, max_n, splits, al, be, part, pstride, s);
+  else err = launch_cgemm<T, kCN>(kb, nk, max_m, max_n, splits, al, be, part, pstride, s);
   AMA_CUDA_TRY(err);
   return AMA_OK;
 }

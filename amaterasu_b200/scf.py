@@ -10,8 +10,10 @@ orbitals are random_bands seeded 12345 + 991 spin + ik (driver.py:360-369).
 
 Precision policy (``config.engine.precision``): "complex128" is the plain FP64 engine;
 "mixed" runs H.psi, Davidson and the density in complex64 and switches the orbitals to
-complex128 once the density residual falls below ``refine_below``, so the fixed point is
-the FP64 one. Energies, densities, potentials and subspace eigensolves are FP64 always.
+complex128 once the density residual falls below ``refine_below``, or earlier when the
+complex64 iterations stop reducing it (best of the last ``stall_window`` iterations not
+below ``stall_ratio`` times the best before them: the FP32 rounding floor of a large cell
+can sit above ``refine_below``), so the fixed point is the FP64 one. Energies, densities, potentials and subspace eigensolves are FP64 always.
 """
 from __future__ import annotations
 
@@ -196,9 +198,15 @@ def run_scf(system, config: Config | None = None, *, logger=None, wavefunctions=
     eigenvalues = np.zeros((system.nspin, system.nkpoints, nb))
     rho_out = rho_in
     iteration = 0
+    res64 = []  # density residuals of the complex64 iterations
     for iteration in range(1, config.scf.max_steps + 1):
         t_step = time.perf_counter()
-        if policy == "mixed" and orb.dtype == torch.complex64 and residual < config.engine.refine_below:
+        w = config.engine.stall_window
+        stalled = len(res64) > w and min(res64[-w:]) > config.engine.stall_ratio * min(res64[:-w])
+        if policy == "mixed" and orb.dtype == torch.complex64 and (residual < config.engine.refine_below or stalled):
+            # the complex64 fixed point differs from the FP64 one by the FP32 rounding floor:
+            # restart the mixer so that its history does not pull towards the former
+            mixer = create_mixer(config.scf.mixing, system)
             orb.to(torch.complex128)
             eng.reserve("complex128", nb)
         prec_name = "complex64" if orb.dtype == torch.complex64 else "complex128"
@@ -216,7 +224,7 @@ def run_scf(system, config: Config | None = None, *, logger=None, wavefunctions=
                 key = ("_batched_davidson", orb.dtype)
                 bd = getattr(system, "_bd_cache", {}).get(key)
                 if bd is None:
-                    bd = BatchedDavidson(system, nb, orb.dtype)
+                    bd = BatchedDavidson(system, nb, orb.dtype, tensor_cores=config.engine.tc_subspace)
                     system._bd_cache = {**getattr(system, "_bd_cache", {}), key: bd}
                 eps, X, _, _ = bd.run(H, orb.packed[spin], tolerance=tol, max_iterations=maxit, spin=spin)
                 eigenvalues[spin] = eps
@@ -261,6 +269,8 @@ def run_scf(system, config: Config | None = None, *, logger=None, wavefunctions=
         local_e = float((veff.reshape(system.nspin, -1) * rho_out).sum()) * dv
         identity = band_sum - (energies.kinetic + local_e + energies.nonlocal_)
         residual = float((rho_out - rho_in).abs().sum()) * dv / system.nelectrons
+        if orb.dtype == torch.complex64:
+            res64.append(residual)
         energy = energies.free_energy
         delta = energy - previous
         history.append((energy, residual, identity))

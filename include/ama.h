@@ -136,6 +136,24 @@ AMA_API int ama_kbatch_zgemm(int32_t precision, int32_t form, int32_t nk, int32_
                              const AmaKOperand* b, const AmaKOperand* c, const double* alpha,
                              const double* beta, int32_t max_m, int32_t max_n, void* stream);
 
+/* The complex64 forms of ama_kbatch_zgemm on the tensor cores (tcgen05, split-TF32 with
+ * FP32 chains drained into registers every 2 k-blocks and FP64 reduction of the splits):
+ *   form 1 (NC): C = alpha A B^H + beta C with k = -1 (reduction over each k's plane
+ *                waves), A and B per-k blocks, C a small matrix per k;
+ *   form 0 (NN): C = alpha A B + beta C with n = -1 (output columns = plane waves), A a
+ *                small matrix per k, B and C per-k blocks.
+ * max_npw bounds npw (host value: the staging arrays are padded to it). Same products as
+ * ama_kbatch_zgemm (davidson.py/subspace.py GEMMs); other forms or shapes are
+ * AMA_ERR_UNSUPPORTED / AMA_ERR_SHAPE. Stream-ordered; scratch grows on demand. */
+AMA_API int ama_kbatch_zgemm_tc(int32_t form, int32_t nk, int32_t m, int32_t n, int32_t k,
+                                const int32_t* npw, const int64_t* pw_off, const AmaKOperand* a,
+                                const AmaKOperand* b, const AmaKOperand* c, const double* alpha,
+                                const double* beta, int32_t max_npw, void* stream);
+
+/* Error flag of the subspace tensor-core kernels (0 = none; otherwise the code of a bounded
+ * wait that timed out). Synchronous. */
+AMA_API int ama_subspace_tc_status(int32_t* code);
+
 /* Teter-Payne-Allan preconditioning fused with the residual and normalisation:
  *   r = hx - eps*x; t_n = sum_G |x|^2 T_G; out = K(T_G / max(t_n,1e-8)) r / ||.||
  * for the `nrows` rows listed in `rows` (device int32); norms (device FP64 [nbands]) get
