@@ -10,12 +10,13 @@
 //             Q_r = P stored interleaved, DxT the real expansion of D.B; written straight
 //             into the interleaved hpsi rows (accumulating onto the FFT result).
 //
-// The operands carry a split-TF32 (hi, lo) pair; the tensor-core kernel adds
-// hi.hi + hi.lo + lo.hi in FP32 (tc_gemm.cuh). Layouts in HBM (FP32, zero padded):
+// The operands carry a split-TF32 (hi, lo) pair; the tensor-core kernel (tc_chain.cuh) adds
+// hi.hi + hi.lo + lo.hi with its FP32 accumulator drained into registers every 2 k-blocks;
+// the projection's reduction splits are summed in FP64. Layouts in HBM (FP32, zero padded):
 //   Bx  [nk][p2][kp]   DxT [nk][mp][k2]   psi [k_count][nbp][kp]   Q [k_count][nbp][k2]
 #include "common.cuh"
 #include "engine_impl.cuh"
-#include "tc_gemm.cuh"
+#include "tc_chain.cuh"
 
 #include <cudaTypedefs.h>
 
@@ -95,196 +96,24 @@ __global__ void split_psi_kernel(const float* __restrict__ psi, const int64_t* _
   }
 }
 
-// partial [kl][split][nbp][p2] -> Q split copies [kl][nbp][k2]; Q[m][2p+d] = D1[d*nproj+p][m].
+// partial [kl][split][nbp][p2] -> Q split copies [kl][nbp][k2]; Q[m][2p+d] = D1[d*nproj+p][m]
+// (splits summed in FP64).
 __global__ void reduce_q_kernel(const float* __restrict__ part, int splits, int nbp, int p2, int k2, int nproj,
                                 float* hi, float* lo) {
   const int kl = blockIdx.z;
   const int m = blockIdx.y;
   for (int j = threadIdx.x; j < k2; j += blockDim.x) {
-    float v = 0.f;
+    double acc = 0.0;
     if (j < 2 * nproj) {
       const int p = j >> 1, d = j & 1;
       const int row = d * nproj + p;
-      for (int s = 0; s < splits; ++s) v += part[(((int64_t)kl * splits + s) * nbp + m) * p2 + row];
+      for (int s = 0; s < splits; ++s) acc += part[(((int64_t)kl * splits + s) * nbp + m) * p2 + row];
     }
+    const float v = (float)acc;
     float a, r;
     tf32_split(v, a, r);
     hi[((int64_t)kl * nbp + m) * k2 + j] = a;
     lo[((int64_t)kl * nbp + m) * k2 + j] = r;
-  }
-}
-
-// ------------------------------------------------------------------ GEMM
-struct TcArgs {
-  int kblocks;     // K / 32 of the whole reduction
-  int splits;      // K splits (project) or 1 (apply)
-  int bn;          // N tile (multiple of 16, <= 256)
-  int n_valid;     // valid N (bands)
-  int stages;
-  int k_first;     // engine k of z = 0 (for the A operand maps that span all k)
-  // mode 0: partial[kl][split][nbp][p2] (column-major tile store)
-  float* part;
-  int nbp, p2;
-  // mode 1: hpsi interleaved accumulate
-  float* out;
-  const int64_t* pw_off;
-  const int* npw;
-  int nbands;
-  int* err;
-};
-
-template <int MODE>
-__global__ void __launch_bounds__(kThreads, 1)
-tc_gemm_kernel(const __grid_constant__ CUtensorMap a_hi, const __grid_constant__ CUtensorMap a_lo,
-               const __grid_constant__ CUtensorMap b_hi, const __grid_constant__ CUtensorMap b_lo, TcArgs p) {
-  extern __shared__ __align__(1024) unsigned char smem_dyn[];
-  __shared__ __align__(8) uint64_t full_bar[kMaxStages], empty_bar[kMaxStages], done_bar;
-  __shared__ uint32_t tmem_slot;
-
-  // 1024-byte aligned operand ring
-  unsigned char* base = reinterpret_cast<unsigned char*>(
-      (reinterpret_cast<uintptr_t>(smem_dyn) + 1023) & ~static_cast<uintptr_t>(1023));
-  const int a_bytes = kBM * kBK * 4;
-  const int b_bytes = p.bn * kBK * 4;
-  const int stage_bytes = 2 * a_bytes + 2 * b_bytes;
-
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int mt = blockIdx.x, nt = blockIdx.y;
-  const int kl = blockIdx.z / p.splits, split = blockIdx.z % p.splits;
-  const int per = (p.kblocks + p.splits - 1) / p.splits;
-  const int kb0 = split * per;
-  const int nkb = max(0, min(p.kblocks, kb0 + per) - kb0);
-  uint32_t ncols = 32;
-  while ((int)ncols < p.bn) ncols <<= 1;
-
-  if (threadIdx.x == 0) {
-    for (int s = 0; s < p.stages; ++s) {
-      mbar_init(&full_bar[s], 1);
-      mbar_init(&empty_bar[s], 1);
-    }
-    mbar_init(&done_bar, 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  if (warp == 2) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
-                 "r"(ncols));
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
-    asm volatile("tcgen05.fence::before_thread_sync;");
-  }
-  __syncthreads();
-  asm volatile("tcgen05.fence::after_thread_sync;");
-  const uint32_t tmem = tmem_slot;
-  bool ok = true;
-
-  if (warp == 0 && lane == 0 && nkb > 0) {
-    // ---------------- TMA producer
-    const int zA = p.k_first + kl;
-    for (int i = 0; i < nkb && ok; ++i) {
-      const int s = i % p.stages;
-      if (i >= p.stages && !mbar_wait(&empty_bar[s], ((i / p.stages) & 1) ^ 1)) {
-        ok = false;
-        atomicExch(p.err, 1);
-        break;
-      }
-      unsigned char* st = base + s * stage_bytes;
-      mbar_expect_tx(&full_bar[s], stage_bytes);
-      const int x = (kb0 + i) * kBK;
-      tma_load_3d(st, &a_hi, &full_bar[s], x, mt * kBM, zA);
-      tma_load_3d(st + a_bytes, &a_lo, &full_bar[s], x, mt * kBM, zA);
-      tma_load_3d(st + 2 * a_bytes, &b_hi, &full_bar[s], x, nt * p.bn, kl);
-      tma_load_3d(st + 2 * a_bytes + b_bytes, &b_lo, &full_bar[s], x, nt * p.bn, kl);
-    }
-  } else if (warp == 1 && lane == 0 && nkb > 0) {
-    // ---------------- MMA issuer
-    const uint32_t idesc = idesc_tf32(p.bn);
-    for (int i = 0; i < nkb; ++i) {
-      const int s = i % p.stages;
-      if (!mbar_wait(&full_bar[s], (i / p.stages) & 1)) {
-        atomicExch(p.err, 2);
-        break;
-      }
-      asm volatile("tcgen05.fence::after_thread_sync;");
-      unsigned char* st = base + s * stage_bytes;
-      const uint64_t ah = smem_desc(st), al = smem_desc(st + a_bytes);
-      const uint64_t bh = smem_desc(st + 2 * a_bytes), bl = smem_desc(st + 2 * a_bytes + b_bytes);
-#pragma unroll
-      for (int kk = 0; kk < kBK / 8; ++kk) {
-        const uint64_t off = (uint64_t)(kk * 32) >> 4;  // 8 TF32 = 32 bytes along K
-        mma_tf32(tmem, ah + off, bh + off, idesc, (i | kk) != 0);
-        mma_tf32(tmem, ah + off, bl + off, idesc, 1);
-        mma_tf32(tmem, al + off, bh + off, idesc, 1);
-      }
-      mma_commit(&empty_bar[s]);
-    }
-    mma_commit(&done_bar);
-  }
-  __syncwarp();
-
-  // ---------------- epilogue: TMEM -> registers -> global
-  bool have = nkb > 0;
-  if (have) {
-    if (!mbar_wait(&done_bar, 0)) {
-      atomicExch(p.err, 3);
-      have = false;
-    }
-  }
-  asm volatile("tcgen05.fence::after_thread_sync;");
-  const int row = mt * kBM + warp * 32 + lane;
-  const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
-  if (MODE == 0) {
-    float* dst = p.part + ((int64_t)kl * p.splits + split) * (int64_t)p.nbp * p.p2;
-    for (int c0 = 0; c0 < p.bn; c0 += 8) {
-      float v[8];
-      if (have) {
-        tmem_ld8(trow + c0, v);
-      } else {
-#pragma unroll
-        for (int t = 0; t < 8; ++t) v[t] = 0.f;
-      }
-#pragma unroll
-      for (int t = 0; t < 8; ++t) {
-        const int col = nt * p.bn + c0 + t;
-        if (col < p.nbp && row < p.p2) dst[(int64_t)col * p.p2 + row] = v[t];
-      }
-    }
-  } else if (have) {
-    // hpsi[m][row] += D[row][m]: 32 columns per round so that 32 independent loads of the
-    // FFT result are in flight per thread before the adds and stores.
-    const int k = p.k_first + kl;
-    const int ld = 2 * p.npw[k];
-    float* __restrict__ outk = p.out + 2 * (p.pw_off[k] - p.pw_off[p.k_first]) * p.nbands;
-    const bool row_ok = row < ld;
-    for (int c0 = 0; c0 < p.bn; c0 += 32) {
-      float v[32];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        float w[8];
-        if (c0 + 8 * q < p.bn) {
-          tmem_ld8(trow + c0 + 8 * q, w);
-        } else {
-#pragma unroll
-          for (int t = 0; t < 8; ++t) w[t] = 0.f;
-        }
-#pragma unroll
-        for (int t = 0; t < 8; ++t) v[8 * q + t] = w[t];
-      }
-      float old[32];
-#pragma unroll
-      for (int t = 0; t < 32; ++t) {
-        const int m = nt * p.bn + c0 + t;
-        old[t] = (row_ok && c0 + t < p.bn && m < p.n_valid) ? outk[(int64_t)m * ld + row] : 0.f;
-      }
-#pragma unroll
-      for (int t = 0; t < 32; ++t) {
-        const int m = nt * p.bn + c0 + t;
-        if (row_ok && c0 + t < p.bn && m < p.n_valid) outk[(int64_t)m * ld + row] = old[t] + v[t];
-      }
-    }
-  }
-  __syncthreads();
-  if (warp == 2) {
-    asm volatile("tcgen05.fence::after_thread_sync;");
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
   }
 }
 
@@ -326,18 +155,6 @@ int grow(float** p, size_t* have, size_t need) {
   return AMA_OK;
 }
 
-// dynamic shared memory: the operand ring plus 1 KB of alignment slack, under the 227 KB
-// per-CTA limit minus the kernel's static barriers
-constexpr int kSmemCap = 227 * 1024 - 1024;
-
-size_t smem_bytes(int bn, int stages) { return (size_t)stages * (2 * kBM * kBK * 4 + 2 * bn * kBK * 4) + 1024; }
-
-int pick_stages(int bn) {
-  int s = kMaxStages;
-  while (s > 2 && smem_bytes(bn, s) > (size_t)kSmemCap) --s;
-  return s;
-}
-
 }  // namespace
 
 namespace ama {
@@ -371,8 +188,10 @@ int nl_tc_setup(AmaEngine* e) {
     if (!rc) rc = make_map(&t.map_dxt[h], t.dxt[h], t.k2, t.mp, e->nk, kBM);
     if (rc) return rc;
   }
-  AMA_CUDA_TRY(cudaFuncSetAttribute(tc_gemm_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemCap));
-  AMA_CUDA_TRY(cudaFuncSetAttribute(tc_gemm_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemCap));
+  AMA_CUDA_TRY(cudaFuncSetAttribute(tc_chain_kernel<kChainPartial>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    kChainSmemCap));
+  AMA_CUDA_TRY(cudaFuncSetAttribute(tc_chain_kernel<kChainAddRows>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    kChainSmemCap));
   t.ready = true;
   return AMA_OK;
 }
@@ -396,12 +215,12 @@ int nl_tc_run(AmaEngine* e, int k_first, int k_count, int nbands, const float2* 
   t.q[1] = t.q[0] + q_half;
   const int kblocks = t.kp / kBK;
   const int mtiles1 = t.p2 / kBM;
-  // Each CTA accumulates at most kChainBlocks k-blocks in tensor memory: the tensor cores
-  // add into the FP32 accumulator with truncation, whose error grows with the chain length;
-  // the split partial sums are then added in FP32 with round-to-nearest by the reduction.
-  constexpr int kChainBlocks = 16;
+  // enough splits to fill the GPU twice, and at most 96 drained chains summed in FP32
+  // registers per CTA
+  constexpr int kMaxChainsPerCta = 96;
+  const int chains = (kblocks + kChain - 1) / kChain;
   int splits = std::max(1, (2 * 148 + mtiles1 * ntile * k_count - 1) / (mtiles1 * ntile * k_count));
-  splits = std::max(splits, (kblocks + kChainBlocks - 1) / kChainBlocks);
+  splits = std::max(splits, (chains + kMaxChainsPerCta - 1) / kMaxChainsPerCta);
   splits = std::min(splits, kblocks);
   rc = grow(&t.part, &t.part_bytes, (size_t)k_count * splits * nbp * t.p2 * sizeof(float));
   if (rc) return rc;
@@ -420,41 +239,41 @@ int nl_tc_run(AmaEngine* e, int k_first, int k_count, int nbands, const float2* 
                                       t.psi[0], t.psi[1]);
   AMA_CHECK_LAUNCH();
 
-  TcArgs a{};
+  ChainArgs a{};
   a.kblocks = kblocks;
   a.splits = splits;
   a.bn = bn;
-  a.n_valid = nbands;
-  a.stages = pick_stages(bn);
-  a.k_first = k_first;
+  a.stages = chain_stages(bn);
+  a.a_z0 = k_first;
   a.part = t.part;
-  a.nbp = nbp;
-  a.p2 = t.p2;
+  a.nrows = t.p2;
+  a.ncols = nbp;
   a.err = t.err;
-  dim3 g1(mtiles1, ntile, k_count * splits);
-  tc_gemm_kernel<0><<<g1, kThreads, smem_bytes(bn, a.stages), s>>>(t.map_bx[0], t.map_bx[1], t.map_psi[0],
-                                                                   t.map_psi[1], a);
+  dim3 g1(ntile, mtiles1, k_count * splits);
+  tc_chain_kernel<kChainPartial><<<g1, kChainThreads, chain_smem(bn, a.stages), s>>>(t.map_bx[0], t.map_bx[1],
+                                                                                     t.map_psi[0], t.map_psi[1], a);
   AMA_CHECK_LAUNCH();
 
   dim3 gr(1, nbp, k_count);
   reduce_q_kernel<<<gr, 256, 0, s>>>(t.part, splits, nbp, t.p2, t.k2, e->nproj, t.q[0], t.q[1]);
   AMA_CHECK_LAUNCH();
 
-  TcArgs b{};
+  ChainArgs b{};
   b.kblocks = t.k2 / kBK;
   b.splits = 1;
   b.bn = bn;
-  b.n_valid = nbands;
-  b.stages = pick_stages(bn);
-  b.k_first = k_first;
+  b.stages = chain_stages(bn);
+  b.a_z0 = k_first;
   b.out = (float*)hpsi;
   b.pw_off = e->d.pw_off;
   b.npw = e->d.npw;
+  b.k_first = k_first;
   b.nbands = nbands;
+  b.n_valid = nbands;
   b.err = t.err;
-  dim3 g2(t.mp / kBM, ntile, k_count);
-  tc_gemm_kernel<1><<<g2, kThreads, smem_bytes(bn, b.stages), s>>>(t.map_dxt[0], t.map_dxt[1], t.map_q[0],
-                                                                   t.map_q[1], b);
+  dim3 g2(ntile, t.mp / kBM, k_count);
+  tc_chain_kernel<kChainAddRows><<<g2, kChainThreads, chain_smem(bn, b.stages), s>>>(t.map_dxt[0], t.map_dxt[1],
+                                                                                     t.map_q[0], t.map_q[1], b);
   AMA_CHECK_LAUNCH();
   return AMA_OK;
 }

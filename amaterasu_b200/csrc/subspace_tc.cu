@@ -17,18 +17,12 @@
 //            coalesced along g.
 //
 // Operands are staged once per call into padded FP32 arrays split into a TF32-exact "hi"
-// and a TF32 "lo" remainder; the MMA adds hi.hi + hi.lo + lo.hi. Accuracy: the tensor
-// cores accumulate in FP32 with truncation, so the accumulator is restarted every kChain
-// k-blocks (24 products per element) and drained into FP32 registers by the epilogue warps
-// (round to nearest) while the MMAs continue into the other of two TMEM buffers; long
-// reductions are additionally split across CTAs and the splits summed in FP64.
-//
-// CTA roles (192 threads): warp 0 lane 0 issues TMA loads (no multicast), warp 1 allocates
-// tensor memory and lane 0 issues the MMAs, warps 2-5 drain and write (warp w reads TMEM
-// lanes 32 (w % 4) .. +31). Every mbarrier wait is bounded; on timeout the CTA records an
-// error code in a device flag (read by ama_subspace_tc_status) and skips ahead to teardown.
+// and a TF32 "lo" remainder; the GEMM (tc_chain.cuh) adds hi.hi + hi.lo + lo.hi with its
+// accumulator drained into registers every 2 k-blocks; long reductions are additionally
+// split across CTAs and the splits summed in FP64. Timeouts of the kernel's bounded waits
+// are reported by ama_subspace_tc_status.
 #include "common.cuh"
-#include "tc_gemm.cuh"
+#include "tc_chain.cuh"
 
 #include <cudaTypedefs.h>
 
@@ -40,32 +34,18 @@ using namespace ama::tc;
 
 namespace {
 
-constexpr int kStThreads = 192;
-constexpr int kStStages = 3;
-constexpr int kStBN = 128;   // N tile (columns of D) at most
-constexpr int kChain = 2;    // k-blocks per tensor-memory accumulation chain
 constexpr int kMaxChainsPerCta = 96;
 
 inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
 
-struct KOpDev {
-  const float* base;  // interleaved complex64 storage viewed as floats
-  int64_t rows_per_k, row0, ld, kstride;
-  int ragged;
-};
+using KOpDev = ChainOp;
 
 KOpDev to_dev(const AmaKOperand* o) {
   return KOpDev{(const float*)o->base, o->rows_per_k, o->row0, o->ld, o->kstride, o->ragged};
 }
 
-// first row of operand `o` at k-point z, and its row length in complex elements
 __device__ __forceinline__ const float* op_rows(const KOpDev& o, int z, int np, int64_t po, int64_t& ld) {
-  if (o.ragged) {
-    ld = np;
-    return o.base + 2 * (o.rows_per_k * po + o.row0 * np);
-  }
-  ld = o.ld;
-  return o.base + 2 * (z * o.kstride + o.row0 * o.ld);
+  return chain_rows(o, z, np, po, ld);
 }
 
 // ------------------------------------------------------------------ staging kernels
@@ -165,202 +145,6 @@ __global__ void stage_nn_r_kernel(KOpDev a, const int* __restrict__ npw, const i
   }
 }
 
-// ------------------------------------------------------------------ GEMM
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
-  uint32_t r[32];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-      "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-      : "r"(taddr));
-#pragma unroll
-  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
-}
-
-struct StArgs {
-  int kblocks;  // k-blocks of the whole reduction
-  int splits;   // reduction splits (grid z = k-point * splits + split)
-  int bn;       // N tile, multiple of 16, <= kStBN
-  // NC: FP32 partial tiles, column-major [z][ncols][nrows]
-  float* part;
-  int nrows, ncols;
-  // NN: complex64 output
-  KOpDev c;
-  const int* npw;
-  const int64_t* pw_off;
-  int m;
-  float2 alpha, beta;
-  int* err;
-};
-
-template <int MODE>  // 0 = NC partials, 1 = NN output
-__global__ void __launch_bounds__(kStThreads, 1)
-subspace_tc_kernel(const __grid_constant__ CUtensorMap a_hi, const __grid_constant__ CUtensorMap a_lo,
-                   const __grid_constant__ CUtensorMap b_hi, const __grid_constant__ CUtensorMap b_lo, StArgs p) {
-  extern __shared__ __align__(1024) unsigned char smem_dyn[];
-  __shared__ __align__(8) uint64_t full_bar[kStStages], empty_bar[kStStages], tfull[2], tempty[2];
-  __shared__ uint32_t tmem_slot;
-
-  unsigned char* base = reinterpret_cast<unsigned char*>(
-      (reinterpret_cast<uintptr_t>(smem_dyn) + 1023) & ~static_cast<uintptr_t>(1023));
-  const int a_bytes = kBM * kBK * 4;
-  const int b_bytes = p.bn * kBK * 4;
-  const int stage_bytes = 2 * a_bytes + 2 * b_bytes;
-
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nt = blockIdx.x, mt = blockIdx.y;
-  const int kz = blockIdx.z / p.splits, split = blockIdx.z % p.splits;
-  const int per = (p.kblocks + p.splits - 1) / p.splits;
-  const int kb0 = split * per;
-  const int nkb = max(0, min(p.kblocks, kb0 + per) - kb0);
-  const int nchains = (nkb + kChain - 1) / kChain;
-  uint32_t ncols = 32;
-  while ((int)ncols < 2 * p.bn) ncols <<= 1;
-
-  if (threadIdx.x == 0) {
-    for (int s = 0; s < kStStages; ++s) {
-      mbar_init(&full_bar[s], 1);
-      mbar_init(&empty_bar[s], 1);
-    }
-    for (int b = 0; b < 2; ++b) {
-      mbar_init(&tfull[b], 1);
-      mbar_init(&tempty[b], 4);
-    }
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  if (warp == 1) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
-                 "r"(ncols));
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
-    asm volatile("tcgen05.fence::before_thread_sync;");
-  }
-  __syncthreads();
-  asm volatile("tcgen05.fence::after_thread_sync;");
-  const uint32_t tmem = tmem_slot;
-
-  if (warp == 0) {
-    if (lane == 0) {
-      for (int i = 0; i < nkb; ++i) {
-        const int s = i % kStStages;
-        if (i >= kStStages && !mbar_wait(&empty_bar[s], ((i / kStStages) & 1) ^ 1)) {
-          atomicExch(p.err, 11);
-          break;
-        }
-        unsigned char* st = base + s * stage_bytes;
-        mbar_expect_tx(&full_bar[s], stage_bytes);
-        const int x = (kb0 + i) * kBK;
-        tma_load_3d(st, &a_hi, &full_bar[s], x, mt * kBM, kz);
-        tma_load_3d(st + a_bytes, &a_lo, &full_bar[s], x, mt * kBM, kz);
-        tma_load_3d(st + 2 * a_bytes, &b_hi, &full_bar[s], x, nt * p.bn, kz);
-        tma_load_3d(st + 2 * a_bytes + b_bytes, &b_lo, &full_bar[s], x, nt * p.bn, kz);
-      }
-    }
-  } else if (warp == 1) {
-    if (lane == 0) {
-      const uint32_t idesc = idesc_tf32(p.bn);
-      for (int i = 0; i < nkb; ++i) {
-        const int c = i / kChain, buf = c & 1;
-        const bool first = (i % kChain) == 0;
-        if (first && c >= 2 && !mbar_wait(&tempty[buf], ((c >> 1) - 1) & 1)) {
-          atomicExch(p.err, 12);
-          break;
-        }
-        const int s = i % kStStages;
-        if (!mbar_wait(&full_bar[s], (i / kStStages) & 1)) {
-          atomicExch(p.err, 13);
-          break;
-        }
-        asm volatile("tcgen05.fence::after_thread_sync;");
-        unsigned char* st = base + s * stage_bytes;
-        const uint64_t ah = smem_desc(st), al = smem_desc(st + a_bytes);
-        const uint64_t bh = smem_desc(st + 2 * a_bytes), bl = smem_desc(st + 2 * a_bytes + b_bytes);
-        const uint32_t td = tmem + (uint32_t)(buf * p.bn);
-#pragma unroll
-        for (int kk = 0; kk < kBK / 8; ++kk) {
-          const uint64_t off = (uint64_t)(kk * 32) >> 4;
-          mma_tf32(td, ah + off, bh + off, idesc, (first && kk == 0) ? 0u : 1u);
-          mma_tf32(td, ah + off, bl + off, idesc, 1);
-          mma_tf32(td, al + off, bh + off, idesc, 1);
-        }
-        mma_commit(&empty_bar[s]);
-        if ((i % kChain) == kChain - 1 || i == nkb - 1) mma_commit(&tfull[buf]);
-      }
-    }
-  } else {
-    // ---------------- epilogue warps: drain chains into registers, then write
-    const int q = warp & 3;
-    const int row = mt * kBM + q * 32 + lane;
-    const uint32_t tlane = tmem + ((uint32_t)(q * 32) << 16);
-    float acc[kStBN];
-#pragma unroll
-    for (int t = 0; t < kStBN; ++t) acc[t] = 0.f;
-    for (int c = 0; c < nchains; ++c) {
-      const int buf = c & 1;
-      if (!mbar_wait(&tfull[buf], (c >> 1) & 1)) {
-        atomicExch(p.err, 14);
-        break;
-      }
-      asm volatile("tcgen05.fence::after_thread_sync;");
-#pragma unroll
-      for (int c0 = 0; c0 < kStBN; c0 += 32) {
-        if (c0 < p.bn) {
-          float v[32];
-          tmem_ld32(tlane + (uint32_t)(buf * p.bn + c0), v);
-          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-          for (int t = 0; t < 32; ++t) acc[c0 + t] += v[t];
-        }
-      }
-      asm volatile("tcgen05.fence::before_thread_sync;");
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&tempty[buf]);
-    }
-    if (MODE == 0) {
-      float* dst = p.part + (int64_t)blockIdx.z * p.ncols * p.nrows;
-#pragma unroll
-      for (int t = 0; t < kStBN; ++t) {
-        const int col = nt * p.bn + t;
-        if (t < p.bn && col < p.ncols && row < p.nrows) dst[(int64_t)col * p.nrows + row] = acc[t];
-      }
-    } else {
-      const int np = p.npw[kz];
-      if (row < np) {
-        int64_t ld;
-        float2* outk = const_cast<float2*>(
-            reinterpret_cast<const float2*>(op_rows(p.c, kz, np, p.pw_off[kz], ld)));
-        const bool use_beta = p.beta.x != 0.f || p.beta.y != 0.f;
-#pragma unroll
-        for (int t = 0; t < kStBN; t += 2) {
-          const int r = (nt * p.bn + t) >> 1;
-          if (t < p.bn && r < p.m) {
-            const float re = acc[t], im = acc[t + 1];
-            float2 o = make_float2(p.alpha.x * re - p.alpha.y * im, p.alpha.x * im + p.alpha.y * re);
-            float2* d = outk + (int64_t)r * ld + row;
-            if (use_beta) {
-              const float2 old = *d;
-              o.x += p.beta.x * old.x - p.beta.y * old.y;
-              o.y += p.beta.x * old.y + p.beta.y * old.x;
-            }
-            *d = o;
-          }
-        }
-      }
-    }
-  }
-  __syncthreads();
-  if (warp == 1) {
-    asm volatile("tcgen05.fence::after_thread_sync;");
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
-  }
-}
-
 // NC: C[z][i][j] = alpha (sum_s part[z,s][j][i] + i sum_s part[z,s][j][mpad + i]) + beta C, FP64 sums.
 __global__ void finalize_nc_kernel(const float* __restrict__ part, int splits, int nrows, int ncols, int mpad, int m,
                                    int n, KOpDev c, const int* __restrict__ npw, const int64_t* __restrict__ pw_off,
@@ -436,9 +220,7 @@ struct TcScratch {
 };
 thread_local TcScratch g_tc;
 
-size_t st_smem(int bn) { return (size_t)kStStages * (2 * kBM * kBK * 4 + 2 * bn * kBK * 4) + 1024; }
-
-int tile_n(int cols) { return cols >= kStBN ? kStBN : std::max(16, round_up(cols, 16)); }
+int tile_n(int cols) { return cols >= kChainBN ? kChainBN : std::max(16, round_up(cols, 16)); }
 
 int ensure_err() {
   if (!g_tc.err) {
@@ -447,10 +229,10 @@ int ensure_err() {
   }
   static bool attrs = false;
   if (!attrs) {
-    AMA_CUDA_TRY(cudaFuncSetAttribute(subspace_tc_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)st_smem(kStBN)));
-    AMA_CUDA_TRY(cudaFuncSetAttribute(subspace_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)st_smem(kStBN)));
+    AMA_CUDA_TRY(cudaFuncSetAttribute(tc_chain_kernel<kChainPartial>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      kChainSmemCap));
+    AMA_CUDA_TRY(cudaFuncSetAttribute(tc_chain_kernel<kChainComplexNN>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, kChainSmemCap));
     attrs = true;
   }
   return AMA_OK;
@@ -487,16 +269,17 @@ int run_nc(int nk, int m, int n, const int32_t* npw, const int64_t* pw_off, cons
   if (!rc) rc = make_map(&mbh, bhi, kp, npad, nk, bn);
   if (!rc) rc = make_map(&mbl, blo, kp, npad, nk, bn);
   if (rc) return rc;
-  StArgs args{};
+  ChainArgs args{};
   args.kblocks = kblocks;
   args.splits = splits;
   args.bn = bn;
+  args.stages = chain_stages(bn);
   args.part = g_tc.part.p;
   args.nrows = rows_a;
   args.ncols = npad;
   args.err = g_tc.err;
-  subspace_tc_kernel<0><<<dim3(npad / bn, rows_a / kBM, nk * splits), kStThreads, st_smem(bn), s>>>(mah, mal, mbh,
-                                                                                                  mbl, args);
+  tc_chain_kernel<kChainPartial><<<dim3(npad / bn, rows_a / kBM, nk * splits), kChainThreads,
+                                   chain_smem(bn, args.stages), s>>>(mah, mal, mbh, mbl, args);
   AMA_CHECK_LAUNCH();
   const int fin_blocks = std::max(1, std::min(1024, (m * n + 255) / 256));
   finalize_nc_kernel<<<dim3(fin_blocks, nk), 256, 0, s>>>(g_tc.part.p, splits, rows_a, npad, mpad, m, n, cd, npw,
@@ -531,10 +314,11 @@ int run_nn(int nk, int m, int kdim, const int32_t* npw, const int64_t* pw_off, c
   if (!rc) rc = make_map(&mbh, bhi, kp, rpad, nk, bn);
   if (!rc) rc = make_map(&mbl, blo, kp, rpad, nk, bn);
   if (rc) return rc;
-  StArgs args{};
+  ChainArgs args{};
   args.kblocks = kp / kBK;
   args.splits = 1;
   args.bn = bn;
+  args.stages = chain_stages(bn);
   args.c = cd;
   args.npw = npw;
   args.pw_off = pw_off;
@@ -542,7 +326,8 @@ int run_nn(int nk, int m, int kdim, const int32_t* npw, const int64_t* pw_off, c
   args.alpha = make_float2((float)alpha[0], (float)alpha[1]);
   args.beta = make_float2((float)beta[0], (float)beta[1]);
   args.err = g_tc.err;
-  subspace_tc_kernel<1><<<dim3(rpad / bn, gpad / kBM, nk), kStThreads, st_smem(bn), s>>>(mah, mal, mbh, mbl, args);
+  tc_chain_kernel<kChainComplexNN><<<dim3(rpad / bn, gpad / kBM, nk), kChainThreads, chain_smem(bn, args.stages),
+                                     s>>>(mah, mal, mbh, mbl, args);
   AMA_CHECK_LAUNCH();
   return AMA_OK;
 }

@@ -215,7 +215,7 @@ def run_scf(system, config: Config | None = None, *, logger=None, wavefunctions=
         H = Hamiltonian(system, veff, precision=prec_name)
         tol = float(np.clip(1e-3 * min(residual, 1.0), 1e-11, 1e-6))
         if orb.dtype == torch.complex64:
-            tol = max(tol, 1e-5)  # below ~1e-5 an FP32 residual is rounding noise
+            tol = max(tol, config.engine.c64_tolerance_floor)  # FP32 residuals carry rounding noise
         maxit = 40 if iteration == 1 else 20
         eigenvalues = np.empty((system.nspin, system.nkpoints, nb))
         for spin in range(system.nspin):
