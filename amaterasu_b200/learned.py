@@ -113,7 +113,7 @@ class DensityNet:
         return self.params[name][0].to(torch.bfloat16).contiguous()
 
     def forward(self, x: torch.Tensor, keep: bool = False):
-        """x: [B][8][36][36][36] FP32 -> Delta [B][1][36]^3 FP32."""
+        """x: [B][8][n][n][n] FP32 (n a multiple of 4) -> Delta [B][1][n]^3 FP32."""
         cache = {}
         w = {name: self._w16(name) for name, *_ in LAYERS}
         b = {name: self.params[name][1] for name, *_ in LAYERS}
@@ -233,7 +233,7 @@ def strain_of(cell, reference_cell) -> np.ndarray:
 
 
 def network_input(n0_work: np.ndarray, strain: np.ndarray) -> np.ndarray:
-    """[8][36]^3 input channels from n0 on the working grid and the strain."""
+    """[8][n]^3 input channels from n0 on the working grid and the strain."""
     x = np.zeros((IN_CHANNELS, *n0_work.shape), dtype=np.float32)
     x[0] = n0_work / max(float(n0_work.mean()), 1e-30)
     for i in range(6):
@@ -247,19 +247,32 @@ def finalize(density: np.ndarray, nelectrons: float, dv: float) -> np.ndarray:
     return d * (nelectrons / (float(d.sum()) * dv))
 
 
+def working_grid(cell, spacing: float) -> int:
+    """Edge of the cubic working grid whose point spacing along the longest cell vector is
+    closest to ``spacing`` (same length unit as ``cell``), rounded to a multiple of 4 (two
+    stride-2 levels). The network is fully convolutional, so a net trained at one spacing
+    runs on larger cells at the same spacing."""
+    length = float(np.max(np.linalg.norm(np.asarray(cell, float), axis=1)))
+    return max(4, int(round(length / spacing / 4.0)) * 4)
+
+
 @dataclass
 class LearnedStart:
-    """Predicts a start density for a system; falls back to the superposition."""
+    """Predicts a start density for a system; falls back to the superposition.
+
+    ``grid`` is the working-grid edge (``WORK_GRID`` for the cells the net was trained on;
+    :func:`working_grid` keeps the training spacing on a larger cell)."""
 
     net: DensityNet
     reference_cell: np.ndarray
     stats: dict = field(default_factory=dict)
+    grid: int = WORK_GRID
 
     def predict(self, system) -> np.ndarray:
         n0 = system.initial_density()  # (nspin, ...)
         total0 = n0.sum(axis=0)
         try:
-            work = fourier_resample(total0, (WORK_GRID,) * 3)
+            work = fourier_resample(total0, (self.grid,) * 3)
             strain = strain_of(system.cell, self.reference_cell)
             x = torch.from_numpy(network_input(np.maximum(work, 1e-12), strain)[None]).to(self.net.device)
             delta, _ = self.net.forward(x)

@@ -1,15 +1,24 @@
 """Data generation, training and evaluation of the learned start density.
 
-    python -m amaterasu_b200.learned_pipeline all --train 48 --test 12 --out DIR
+    python -m amaterasu_b200.learned_pipeline all --family si8 --train 48 --test 12 --out DIR
+    python -m amaterasu_b200.learned_pipeline all --family si64 --train 32 --test 4 --out DIR
 
-Cells: the 8-atom conventional silicon cell (a = 5.43 A) under a seeded random symmetric
-strain (components uniform in +-3 %) with seeded N(0, 0.1 A) atomic displacements, the
-synthetic norm-conserving dataset, ecut 30 Ry, an unshifted 4x4x4 mesh reduced by time
-reversal, LDA-PZ, Gaussian smearing 0.01 Ha. Each cell is converged by the engine
-(mixed precision with FP64 refinement) from the superposed atomic density; the pair
-(n0, strain) -> n_conv, resampled to the 36^3 working grid, is one training sample.
-Evaluation converges held-out cells from both starts and reports iterations, time and the
-final-energy difference (the fixed point must not move: |dE| < 1e-6 Ha).
+Cell families (synthetic norm-conserving dataset, ecut 30 Ry, LDA-PZ):
+
+* ``si8``: the 8-atom conventional silicon cell (a = 5.43 A) under a seeded random
+  symmetric strain (components uniform in +-3 %) with seeded N(0, 0.1 A) displacements,
+  an unshifted 4x4x4 mesh reduced by time reversal, Gaussian smearing 0.01 Ha, 20 bands,
+  working grid 36^3.
+* ``si64``: the 2x2x2 conventional supercell (a = 10.86 A) with strain in +-1 %, N(0,
+  0.05 A) displacements and, in every second cell, a vacancy; Gamma only, Gaussian smearing
+  0.005 Ha, 144 bands, working grid 40^3 (0.27 A spacing, which the 3x3x3 supercell reaches
+  at 60^3: the net trained here starts that cell).
+
+Each cell is converged by the engine (mixed precision with FP64 refinement) from the
+superposed atomic density; the pair (n0, strain) -> n_conv on the working grid is one
+training sample. Evaluation converges held-out cells from both starts and reports
+iterations, time and the final-energy difference (the fixed point must not move:
+|dE| < 1e-6 Ha).
 """
 from __future__ import annotations
 
@@ -22,18 +31,36 @@ from pathlib import Path
 import numpy as np
 
 A_SI = 5.43
+BOHR_IN_ANGSTROM = 0.529177210903
+
+FAMILIES = {
+    "si8": dict(supercell=1, strain=0.03, sigma=0.1, vacancy_every=0, kmesh=(4, 4, 4), smearing="0.01 Ha",
+                nbands=20, grid=36),
+    "si64": dict(supercell=2, strain=0.01, sigma=0.05, vacancy_every=2, kmesh=None, smearing="0.005 Ha",
+                 nbands=144, grid=40),
+}
 
 
-def make_cell(seed: int):
+def reference_cell(family: str) -> np.ndarray:
+    """Unstrained cell of a family, Angstrom."""
+    return np.eye(3) * A_SI * FAMILIES[family]["supercell"]
+
+
+def make_cell(seed: int, family: str = "si8"):
     from .cells import _DIAMOND
     from .system import Structure
+    f = FAMILIES[family]
+    n = f["supercell"]
     rng = np.random.default_rng(seed)
-    e = rng.uniform(-0.03, 0.03, size=(3, 3))
+    e = rng.uniform(-f["strain"], f["strain"], size=(3, 3))
     e = 0.5 * (e + e.T)
-    ref = np.eye(3) * A_SI
+    ref = reference_cell(family)
     cell = ref @ (np.eye(3) + e)
-    pos = _DIAMOND @ cell + rng.normal(scale=0.1, size=(8, 3))
-    return Structure(["Si"] * 8, pos, cell), ref
+    frac = np.vstack([(_DIAMOND + np.array([i, j, k])) / n for i in range(n) for j in range(n) for k in range(n)])
+    if f["vacancy_every"] and seed % f["vacancy_every"] == 0:
+        frac = frac[1:]
+    pos = frac @ cell + rng.normal(scale=f["sigma"], size=(len(frac), 3))
+    return Structure(["Si"] * len(pos), pos, cell), ref
 
 
 def _pseudo():
@@ -42,11 +69,11 @@ def _pseudo():
         return read_upf(write_synthetic_upf(Path(tmp) / "Si.upf"))
 
 
-def _config(precision="mixed"):
+def _config(family: str, precision="mixed"):
     from .config import Config
     c = Config()
     c.occupations.scheme = "gaussian"
-    c.occupations.smearing = "0.01 Ha"
+    c.occupations.smearing = FAMILIES[family]["smearing"]
     c.scf.tol_energy = 1e-6
     c.scf.tol_density = 1e-7
     c.scf.max_steps = 60
@@ -54,31 +81,33 @@ def _config(precision="mixed"):
     return c
 
 
-def build(structure, pseudo, kmesh=(4, 4, 4), ecut=15.0):
+def build(structure, pseudo, family: str, ecut=15.0):
     from . import kpoints as kp
     from .system import build_system
-    return build_system(structure, {"Si": pseudo}, ecut, 4 * ecut, kpoints=kp.monkhorst_pack(kmesh), nbands=20)
+    f = FAMILIES[family]
+    kpts = kp.monkhorst_pack(f["kmesh"]) if f["kmesh"] else kp.gamma_only()
+    return build_system(structure, {"Si": pseudo}, ecut, 4 * ecut, kpoints=kpts, nbands=f["nbands"])
 
 
-def run_cell(seed, pseudo, *, kmesh=(4, 4, 4), ecut=15.0, density=None, precision="mixed"):
+def run_cell(seed, pseudo, *, family="si8", ecut=15.0, density=None, precision="mixed"):
     import torch
-    from .learned import WORK_GRID, fourier_resample, strain_of
+    from .learned import fourier_resample, strain_of
     from .scf import run_scf
-    structure, ref = make_cell(seed)
-    system = build(structure, pseudo, kmesh, ecut)
+    structure, ref = make_cell(seed, family)
+    system = build(structure, pseudo, family, ecut)
     n0 = system.initial_density()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     start = n0 if density is None else density(system)
-    res = run_scf(system, _config(precision), density=start)
+    res = run_scf(system, _config(family, precision), density=start)
     torch.cuda.synchronize()
     seconds = time.perf_counter() - t0
-    work = (WORK_GRID,) * 3
+    work = (FAMILIES[family]["grid"],) * 3
     return dict(seed=seed, grid=list(system.grid.shape), iterations=res.iterations, converged=res.converged,
                 free_energy=res.energies.free_energy, seconds=seconds,
                 n0=fourier_resample(n0.sum(0), work).astype(np.float32),
                 nconv=fourier_resample(res.density.sum(0), work).astype(np.float32),
-                strain=strain_of(system.cell, ref * (1.0 / 0.529177210903)))
+                strain=strain_of(system.cell, ref / BOHR_IN_ANGSTROM))
 
 
 def generate(seeds, out_file, **kw):
@@ -112,15 +141,19 @@ def fit(dataset, weights_out, epochs=200, seed=0):
     return hist
 
 
-def evaluate(weights, seeds, **kw):
+def learned_start(weights, family: str):
     from .learned import DensityNet, LearnedStart
-    pseudo = _pseudo()
     net = DensityNet.from_file(weights)
-    learned = LearnedStart(net, np.eye(3) * A_SI / 0.529177210903)
+    return LearnedStart(net, reference_cell(family) / BOHR_IN_ANGSTROM, grid=FAMILIES[family]["grid"])
+
+
+def evaluate(weights, seeds, *, family="si8", **kw):
+    pseudo = _pseudo()
+    learned = learned_start(weights, family)
     rows = []
     for s in seeds:
-        base = run_cell(s, pseudo, **kw)
-        pred = run_cell(s, pseudo, density=learned.predict, **kw)
+        base = run_cell(s, pseudo, family=family, **kw)
+        pred = run_cell(s, pseudo, family=family, density=learned.predict, **kw)
         rows.append(dict(seed=s, iterations_superposition=base["iterations"], iterations_learned=pred["iterations"],
                          seconds_superposition=base["seconds"], seconds_learned=pred["seconds"],
                          energy_difference=abs(base["free_energy"] - pred["free_energy"]),
@@ -129,33 +162,36 @@ def evaluate(weights, seeds, **kw):
     return rows
 
 
+def summarize(rows) -> dict:
+    return dict(cells=len(rows),
+                mean_iterations_superposition=float(np.mean([r["iterations_superposition"] for r in rows])),
+                mean_iterations_learned=float(np.mean([r["iterations_learned"] for r in rows])),
+                mean_seconds_superposition=float(np.mean([r["seconds_superposition"] for r in rows])),
+                mean_seconds_learned=float(np.mean([r["seconds_learned"] for r in rows])),
+                max_energy_difference=float(np.max([r["energy_difference"] for r in rows])),
+                rows=rows)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("stage", choices=["generate", "fit", "evaluate", "all"])
+    ap.add_argument("--family", choices=sorted(FAMILIES), default="si8")
     ap.add_argument("--train", type=int, default=48)
     ap.add_argument("--test", type=int, default=12)
     ap.add_argument("--epochs", type=int, default=200)
-    ap.add_argument("--kmesh", type=int, nargs=3, default=[4, 4, 4])
     ap.add_argument("--out", default="learned_out")
     args = ap.parse_args()
     out = Path(args.out)
     out.mkdir(parents=True, exist_ok=True)
     train_seeds = list(range(1000, 1000 + args.train))
     test_seeds = list(range(5000, 5000 + args.test))
-    kw = dict(kmesh=tuple(args.kmesh))
     if args.stage in ("generate", "all"):
-        generate(train_seeds, out / "dataset.npz", **kw)
+        generate(train_seeds, out / "dataset.npz", family=args.family)
     if args.stage in ("fit", "all"):
         fit(out / "dataset.npz", out / "density_net.npz", epochs=args.epochs)
     if args.stage in ("evaluate", "all"):
-        rows = evaluate(out / "density_net.npz", test_seeds, **kw)
-        summary = dict(cells=len(rows),
-                       mean_iterations_superposition=float(np.mean([r["iterations_superposition"] for r in rows])),
-                       mean_iterations_learned=float(np.mean([r["iterations_learned"] for r in rows])),
-                       mean_seconds_superposition=float(np.mean([r["seconds_superposition"] for r in rows])),
-                       mean_seconds_learned=float(np.mean([r["seconds_learned"] for r in rows])),
-                       max_energy_difference=float(np.max([r["energy_difference"] for r in rows])),
-                       rows=rows)
+        summary = summarize(evaluate(out / "density_net.npz", test_seeds, family=args.family))
+        summary["family"] = args.family
         (out / "evaluation.json").write_text(json.dumps(summary, indent=1))
         print(json.dumps({k: v for k, v in summary.items() if k != "rows"}), flush=True)
 

@@ -1,0 +1,117 @@
+"""SCF wall time of the engine's precision policies on one workload.
+
+    python -m amaterasu_b200.scf_benchmark --workload si215_gamma \\
+        --weights amaterasu_b200/data/density_net_si64.npz --out scf_si215.json
+
+Runs, on the same system and GPU, to |dF| < 1e-5 eV/atom and an integrated density
+residual below 1e-7 per electron:
+
+* ``plain``: the FP64 engine (complex128 H.psi, Davidson and density) from the superposed
+  atomic density, the reference's start;
+* ``mixed``: complex64 bulk with tensor-core subspace products, FP64 refinement, from the
+  same start;
+* ``learned+mixed`` (with ``--weights``): the mixed policy from the learned start density.
+
+Reported per run: SCF seconds (system set-up excluded, the same for every run),
+iterations, free energy, |dF| per atom against the plain run, and the largest force
+difference against the plain run (eV/A) when ``--forces`` is given.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+HARTREE_PER_BOHR_IN_EV_PER_ANG = 27.211386245988 / 0.529177210903
+SMEARING = {"si215_gamma": ("gaussian", "0.005 Ha"), "si8_batched": ("fermi-dirac", "0.01 Ha"),
+            "si2_scf": ("fixed", None), "si64_hpsi": ("gaussian", "0.005 Ha")}
+
+
+def _system(workload: str):
+    from .cells import workload as make
+    from .pseudo import read_upf, write_synthetic_upf
+    from .system import build_system
+    with tempfile.TemporaryDirectory() as tmp:
+        pseudo = read_upf(write_synthetic_upf(Path(tmp) / "Si.upf"))
+    structure, ecut, kpts, nbands = make(workload)
+    return build_system(structure, {"Si": pseudo}, ecut, 4 * ecut, kpoints=kpts, nbands=nbands)
+
+
+def _config(workload: str, precision: str):
+    from .config import Config
+    c = Config()
+    scheme, smearing = SMEARING[workload]
+    c.occupations.scheme = scheme
+    if smearing:
+        c.occupations.smearing = smearing
+    c.scf.tol_energy = 1e-5
+    c.scf.tol_density = 1e-7
+    c.scf.max_steps = 80
+    c.engine.precision = precision
+    return c
+
+
+def run(workload: str, weights=None, forces=False, log=print) -> dict:
+    import torch
+    from .learned import DensityNet, LearnedStart, working_grid
+    from .scf import run_scf
+    t0 = time.perf_counter()
+    system = _system(workload)
+    setup = time.perf_counter() - t0
+    runs = [("plain", "complex128", None), ("mixed", "mixed", None)]
+    if weights:
+        net = DensityNet.from_file(weights)
+        cell = np.asarray(system.cell, float)
+        # the net was trained at a working-grid spacing of 0.27 A (10.86 A cell on 40^3)
+        learned = LearnedStart(net, cell, grid=working_grid(cell, 10.86 / 0.529177210903 / 40))
+        runs.append(("learned+mixed", "mixed", learned))
+    out = dict(workload=workload, setup_seconds=setup, natoms=system.natoms, runs={})
+    results = {}
+    for name, precision, start in runs:
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        density = start.predict(system) if start is not None else None
+        res = run_scf(system, _config(workload, precision), density=density)
+        torch.cuda.synchronize()
+        seconds = time.perf_counter() - t
+        row = dict(seconds=seconds, iterations=res.iterations, converged=res.converged,
+                   free_energy=res.energies.free_energy, precision_trace=res.precision_trace.count("complex64"))
+        if start is not None:
+            row["fallback"] = bool(start.stats.get("fallback", False))
+        if forces:
+            from .properties import compute_forces
+            row["_forces"] = compute_forces(system, res.density, res.wavefunctions, res.occupations)
+        results[name] = row
+        log(f"{name}: {seconds:.1f} s, {res.iterations} iterations, F = {res.energies.free_energy:.10f} Ha")
+    plain = results["plain"]
+    for name, row in results.items():
+        row["dF_per_atom_eV"] = abs(row["free_energy"] - plain["free_energy"]) * 27.211386245988 / system.natoms
+        row["speedup_vs_plain"] = plain["seconds"] / row["seconds"]
+        if forces:
+            row["max_force_diff_eV_per_A"] = float(np.abs(row["_forces"] - plain["_forces"]).max()
+                                                   * HARTREE_PER_BOHR_IN_EV_PER_ANG)
+        row.pop("_forces", None)
+        out["runs"][name] = row
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="si215_gamma", choices=sorted(SMEARING))
+    ap.add_argument("--weights", default=None)
+    ap.add_argument("--forces", action="store_true")
+    ap.add_argument("--out", default=None)
+    args = ap.parse_args()
+    result = run(args.workload, args.weights, args.forces)
+    text = json.dumps(result, indent=1)
+    print(text, flush=True)
+    if args.out:
+        Path(args.out).write_text(text)
+
+
+if __name__ == "__main__":
+    main()

@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--kpoints", type=int, default=4, help="k-points of the workload to include (profiling)")
     ap.add_argument("--no-extras", action="store_true", help="skip the e2e and complex128 legs (profiling)")
+    ap.add_argument("--scf", action="store_true",
+                    help="also time the Si215 Gamma SCF (plain FP64, mixed, learned+mixed; several minutes)")
     return ap.parse_args()
 
 
@@ -321,6 +323,11 @@ def main():
         "clocks": clocks,
         **extra,
     }
+    if args.scf and world == 1:
+        from amaterasu_b200.scf_benchmark import run as scf_run
+        weights = REPO / "amaterasu_b200" / "data" / "density_net_si64.npz"
+        line["scf"] = scf_run("si215_gamma", str(weights) if weights.exists() else None, forces=True,
+                              log=lambda *_: None)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle.potential import hartree, xc_on_grid  # noqa: F401
         veff_np = veff[0].cpu().numpy()

@@ -26,3 +26,24 @@ def test_strain_of_recovers_symmetric_strain():
     full = np.array([[e[0], e[5], e[4]], [e[5], e[1], e[3]], [e[4], e[3], e[2]]])
     np.testing.assert_allclose(ref @ (np.eye(3) + full), s.cell, atol=1e-12)
     assert np.all(np.abs(e) <= 0.03 + 1e-12)
+
+
+def test_working_grid_keeps_the_training_spacing():
+    from amaterasu_b200.learned import working_grid
+    spacing = 10.86 / 40
+    assert working_grid(np.eye(3) * 10.86, spacing) == 40
+    assert working_grid(np.eye(3) * 16.29, spacing) == 60
+    assert working_grid(np.eye(3) * 5.43, 5.43 / 36) == 36
+    assert working_grid(np.eye(3) * 16.29, spacing) % 4 == 0
+
+
+def test_si64_family_cells():
+    from amaterasu_b200.learned import strain_of
+    from amaterasu_b200.learned_pipeline import make_cell
+    a, ref = make_cell(1000, "si64")
+    b, _ = make_cell(1001, "si64")
+    assert {len(a.symbols), len(b.symbols)} == {63, 64}  # a vacancy in every second cell
+    e = strain_of(a.cell, ref)
+    assert np.all(np.abs(e) <= 0.01 + 1e-12)
+    again, _ = make_cell(1000, "si64")
+    np.testing.assert_array_equal(again.positions, a.positions)
