@@ -292,8 +292,13 @@ class LearnedStart:
 
 
 def train(net: DensityNet, inputs: np.ndarray, targets: np.ndarray, *, epochs: int = 200, batch: int = 4,
-          lr: float = 2e-3, seed: int = 0, log=None) -> list:
-    """Fit Delta to log(n_conv / n0) on the working grid (mean squared error)."""
+          lr: float = 2e-3, seed: int = 0, log=None, density_weighted: bool = True) -> list:
+    """Fit Delta to log(n_conv / n0) on the working grid.
+
+    The loss is the mean squared error weighted by n0 / mean(n0) (input channel 0): the
+    start density's error is n0 * dDelta to first order, so low-density regions (vacancies,
+    interstitials), where log(n_conv / n0) is large but carries little charge, do not
+    dominate the fit. ``density_weighted=False`` gives the plain mean squared error."""
     rng = np.random.default_rng(seed)
     x_all = torch.from_numpy(np.asarray(inputs, dtype=np.float32)).to(net.device)
     t_all = torch.from_numpy(np.asarray(targets, dtype=np.float32)).to(net.device)
@@ -307,8 +312,9 @@ def train(net: DensityNet, inputs: np.ndarray, targets: np.ndarray, *, epochs: i
             x, t = x_all[idx], t_all[idx]
             out, cache = net.forward(x, keep=True)
             diff = out - t
-            loss = float((diff * diff).mean())
-            dout = (2.0 / diff.numel()) * diff
+            w = x[:, :1] if density_weighted else torch.ones_like(diff)
+            loss = float((w * diff * diff).mean())
+            dout = (2.0 / diff.numel()) * w * diff
             grads = net.backward(dout.contiguous(), cache)
             step_lr = lr * 0.5 * (1 + np.cos(np.pi * epoch / max(epochs, 1)))
             net.adam_step(grads, lr=step_lr)

@@ -11,8 +11,13 @@ Cell families (synthetic norm-conserving dataset, ecut 30 Ry, LDA-PZ):
   working grid 36^3.
 * ``si64``: the 2x2x2 conventional supercell (a = 10.86 A) with strain in +-1 %, N(0,
   0.05 A) displacements and, in every second cell, a vacancy; Gamma only, Gaussian smearing
-  0.005 Ha, 144 bands, working grid 40^3 (0.27 A spacing, which the 3x3x3 supercell reaches
-  at 60^3: the net trained here starts that cell).
+  0.005 Ha, 144 bands, working grid 72^3 (0.151 A, the spacing of the si8 grid and of the
+  3x3x3 supercell's 108^3 grid: the net trained here starts that cell). Its fit starts from
+  the si8 weights (``fit --init``).
+
+A coarser working grid than the system grid truncates the converged density's Fourier
+series and the ringing makes log(n_conv / n0) meaningless in low-density regions, so the
+working grids keep the system grid's spacing.
 
 Each cell is converged by the engine (mixed precision with FP64 refinement) from the
 superposed atomic density; the pair (n0, strain) -> n_conv on the working grid is one
@@ -37,7 +42,7 @@ FAMILIES = {
     "si8": dict(supercell=1, strain=0.03, sigma=0.1, vacancy_every=0, kmesh=(4, 4, 4), smearing="0.01 Ha",
                 nbands=20, grid=36),
     "si64": dict(supercell=2, strain=0.01, sigma=0.05, vacancy_every=2, kmesh=None, smearing="0.005 Ha",
-                 nbands=144, grid=40),
+                 nbands=144, grid=72),
 }
 
 
@@ -131,12 +136,12 @@ def samples(data):
     return x, t
 
 
-def fit(dataset, weights_out, epochs=200, seed=0):
+def fit(dataset, weights_out, epochs=200, seed=0, lr=2e-3, init=None):
     from .learned import DensityNet, train
     data = np.load(dataset)
     x, t = samples(data)
-    net = DensityNet(seed=seed)
-    hist = train(net, x, t, epochs=epochs, log=lambda m: print(m, flush=True))
+    net = DensityNet.from_file(init) if init else DensityNet(seed=seed)
+    hist = train(net, x, t, epochs=epochs, lr=lr, log=lambda m: print(m, flush=True))
     net.save(weights_out)
     return hist
 
@@ -179,6 +184,8 @@ def main():
     ap.add_argument("--train", type=int, default=48)
     ap.add_argument("--test", type=int, default=12)
     ap.add_argument("--epochs", type=int, default=200)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--init", default=None, help="start the fit from these weights")
     ap.add_argument("--out", default="learned_out")
     args = ap.parse_args()
     out = Path(args.out)
@@ -188,7 +195,7 @@ def main():
     if args.stage in ("generate", "all"):
         generate(train_seeds, out / "dataset.npz", family=args.family)
     if args.stage in ("fit", "all"):
-        fit(out / "dataset.npz", out / "density_net.npz", epochs=args.epochs)
+        fit(out / "dataset.npz", out / "density_net.npz", epochs=args.epochs, lr=args.lr, init=args.init)
     if args.stage in ("evaluate", "all"):
         summary = summarize(evaluate(out / "density_net.npz", test_seeds, family=args.family))
         summary["family"] = args.family

@@ -1,7 +1,7 @@
 """SCF wall time of the engine's precision policies on one workload.
 
     python -m amaterasu_b200.scf_benchmark --workload si215_gamma \\
-        --weights amaterasu_b200/data/density_net_si64.npz --out scf_si215.json
+        --weights amaterasu_b200/data/density_net_si64.npz --forces --out scf_si215.json
 
 Runs, on the same system and GPU, to |dF| < 1e-5 eV/atom and an integrated density
 residual below 1e-7 per electron:
@@ -10,7 +10,8 @@ residual below 1e-7 per electron:
   atomic density, the reference's start;
 * ``mixed``: complex64 bulk with tensor-core subspace products, FP64 refinement, from the
   same start;
-* ``learned+mixed`` (with ``--weights``): the mixed policy from the learned start density.
+* ``learned+mixed`` (with ``--weights``): the mixed policy from the learned start density,
+  the network run on a working grid with the spacing it was trained at (0.151 A).
 
 Reported per run: SCF seconds (system set-up excluded, the same for every run),
 iterations, free energy, |dF| per atom against the plain run, and the largest force
@@ -41,9 +42,11 @@ def _system(workload: str):
     return build_system(structure, {"Si": pseudo}, ecut, 4 * ecut, kpoints=kpts, nbands=nbands)
 
 
-def _config(workload: str, precision: str):
+def _config(workload: str, precision: str, engine_options=None):
     from .config import Config
     c = Config()
+    for key, value in (engine_options or {}).items():
+        setattr(c.engine, key, value)
     scheme, smearing = SMEARING[workload]
     c.occupations.scheme = scheme
     if smearing:
@@ -55,19 +58,22 @@ def _config(workload: str, precision: str):
     return c
 
 
-def run(workload: str, weights=None, forces=False, log=print) -> dict:
+TRAINING_SPACING_A = 5.43 / 36  # working-grid spacing the committed nets were trained at
+
+
+def run(workload: str, weights=None, forces=False, log=print, policies=("plain", "mixed", "learned+mixed"),
+        engine_options=None, spacing=TRAINING_SPACING_A) -> dict:
     import torch
     from .learned import DensityNet, LearnedStart, working_grid
     from .scf import run_scf
     t0 = time.perf_counter()
     system = _system(workload)
     setup = time.perf_counter() - t0
-    runs = [("plain", "complex128", None), ("mixed", "mixed", None)]
-    if weights:
+    runs = [(p, {"plain": "complex128"}.get(p, "mixed"), None) for p in policies if p in ("plain", "mixed")]
+    if weights and "learned+mixed" in policies:
         net = DensityNet.from_file(weights)
         cell = np.asarray(system.cell, float)
-        # the net was trained at a working-grid spacing of 0.27 A (10.86 A cell on 40^3)
-        learned = LearnedStart(net, cell, grid=working_grid(cell, 10.86 / 0.529177210903 / 40))
+        learned = LearnedStart(net, cell, grid=working_grid(cell, spacing / 0.529177210903))
         runs.append(("learned+mixed", "mixed", learned))
     out = dict(workload=workload, setup_seconds=setup, natoms=system.natoms, runs={})
     results = {}
@@ -75,7 +81,7 @@ def run(workload: str, weights=None, forces=False, log=print) -> dict:
         torch.cuda.synchronize()
         t = time.perf_counter()
         density = start.predict(system) if start is not None else None
-        res = run_scf(system, _config(workload, precision), density=density)
+        res = run_scf(system, _config(workload, precision, engine_options), density=density)
         torch.cuda.synchronize()
         seconds = time.perf_counter() - t
         row = dict(seconds=seconds, iterations=res.iterations, converged=res.converged,
@@ -87,16 +93,32 @@ def run(workload: str, weights=None, forces=False, log=print) -> dict:
             row["_forces"] = compute_forces(system, res.density, res.wavefunctions, res.occupations)
         results[name] = row
         log(f"{name}: {seconds:.1f} s, {res.iterations} iterations, F = {res.energies.free_energy:.10f} Ha")
-    plain = results["plain"]
+    plain = results.get("plain")
     for name, row in results.items():
-        row["dF_per_atom_eV"] = abs(row["free_energy"] - plain["free_energy"]) * 27.211386245988 / system.natoms
-        row["speedup_vs_plain"] = plain["seconds"] / row["seconds"]
-        if forces:
-            row["max_force_diff_eV_per_A"] = float(np.abs(row["_forces"] - plain["_forces"]).max()
-                                                   * HARTREE_PER_BOHR_IN_EV_PER_ANG)
-        row.pop("_forces", None)
+        if plain is not None:
+            row["dF_per_atom_eV"] = abs(row["free_energy"] - plain["free_energy"]) * 27.211386245988 / system.natoms
+            row["speedup_vs_plain"] = plain["seconds"] / row["seconds"]
+            if forces:
+                row["max_force_diff_eV_per_A"] = float(np.abs(row["_forces"] - plain["_forces"]).max()
+                                                       * HARTREE_PER_BOHR_IN_EV_PER_ANG)
         out["runs"][name] = row
+    for row in results.values():
+        row.pop("_forces", None)
     return out
+
+
+def parse_engine_options(items) -> dict:
+    """KEY=VALUE strings -> EngineConfig overrides, typed like the defaults."""
+    from .config import EngineConfig
+    defaults = EngineConfig()
+    options = {}
+    for item in items:
+        key, value = item.split("=", 1)
+        if not hasattr(defaults, key):
+            raise ValueError(f"unknown engine option {key!r}")
+        kind = type(getattr(defaults, key))
+        options[key] = value.lower() in ("1", "true", "yes") if kind is bool else kind(value)
+    return options
 
 
 def main():
@@ -104,9 +126,15 @@ def main():
     ap.add_argument("--workload", default="si215_gamma", choices=sorted(SMEARING))
     ap.add_argument("--weights", default=None)
     ap.add_argument("--forces", action="store_true")
+    ap.add_argument("--policies", default="plain,mixed,learned+mixed")
+    ap.add_argument("--spacing", type=float, default=TRAINING_SPACING_A,
+                    help="working-grid spacing (A) the network was trained at")
+    ap.add_argument("--engine", action="append", default=[],
+                    help="engine option override KEY=VALUE (e.g. c64_tolerance_floor=5e-7)")
     ap.add_argument("--out", default=None)
     args = ap.parse_args()
-    result = run(args.workload, args.weights, args.forces)
+    result = run(args.workload, args.weights, args.forces, policies=tuple(args.policies.split(",")),
+                 engine_options=parse_engine_options(args.engine), spacing=args.spacing)
     text = json.dumps(result, indent=1)
     print(text, flush=True)
     if args.out:
