@@ -69,6 +69,10 @@ class EngineConfig:
     # lowest Davidson residual tolerance of the complex64 iterations: the FP32 H.psi and
     # subspace products leave a residual noise of a few 1e-7 Ha
     c64_tolerance_floor: float = 2e-6
+    # Davidson iterations per SCF step once a mixed run has switched to complex128 (0: the
+    # reference's 20); the orbitals enter the refinement converged to the FP32 floor, and
+    # the SCF convergence test is unchanged
+    refine_max_iterations: int = 4
     batched: bool = True
 
 

@@ -39,8 +39,12 @@ cgemm_tile_kernel(Batch batch, int splits, cx_t<T> alpha, cx_t<T> beta, double2*
                   int64_t partial_stride) {
   using C = cx_t<T>;
   constexpr int BK = GemmBK<T>::value;
-  __shared__ C As[BK][kBM + 1];
-  __shared__ C Bs[BK][kBN + 1];
+  constexpr int LA = BK * kBM / kGemmThreads;  // tile elements each thread stages
+  constexpr int LB = BK * kBN / kGemmThreads;
+  // two shared-memory buffers: the next k-tile is loaded into registers while the current
+  // one is multiplied, then stored into the other buffer (one barrier per k-tile)
+  __shared__ C As[2][BK][kBM + 1];
+  __shared__ C Bs[2][BK][kBN + 1];
 
   const int z = blockIdx.z;
   const int bz = z / splits, sz = z % splits;
@@ -67,10 +71,11 @@ cgemm_tile_kernel(Batch batch, int splits, cx_t<T> alpha, cx_t<T> beta, double2*
       for (int j = 0; j < 4; ++j) dacc[i][j] = make_double2(0.0, 0.0);
   }
 
-  int tile_count = 0;
-  for (int k0 = kbeg; k0 < kend; k0 += BK) {
-    // ---- A tile -> As[kk][mm]
-    for (int e = tid; e < BK * kBM; e += kGemmThreads) {
+  C ra[LA], rb[LB];
+  auto load_tile = [&](int k0) {
+#pragma unroll
+    for (int l = 0; l < LA; ++l) {
+      const int e = tid + l * kGemmThreads;
       int mm, kk;
       if (FORM == kCN) { mm = e % kBM; kk = e / kBM; }   // A is (k x m): m contiguous
       else { kk = e % BK; mm = e / BK; }                  // A is (m x k): k contiguous
@@ -80,10 +85,11 @@ cgemm_tile_kernel(Batch batch, int splits, cx_t<T> alpha, cx_t<T> beta, double2*
         if (FORM == kCN) { v = p.a[(int64_t)gk * p.lda + gm]; v.y = -v.y; }
         else v = p.a[(int64_t)gm * p.lda + gk];
       }
-      As[kk][mm] = v;
+      ra[l] = v;
     }
-    // ---- B tile -> Bs[kk][nn]
-    for (int e = tid; e < BK * kBN; e += kGemmThreads) {
+#pragma unroll
+    for (int l = 0; l < LB; ++l) {
+      const int e = tid + l * kGemmThreads;
       int nn, kk;
       if (FORM == kNC) { kk = e % BK; nn = e / BK; }      // B is (n x k): k contiguous
       else { nn = e % kBN; kk = e / kBN; }                // B is (k x n): n contiguous
@@ -93,16 +99,40 @@ cgemm_tile_kernel(Batch batch, int splits, cx_t<T> alpha, cx_t<T> beta, double2*
         if (FORM == kNC) { v = p.b[(int64_t)gn * p.ldb + gk]; v.y = -v.y; }
         else v = p.b[(int64_t)gk * p.ldb + gn];
       }
-      Bs[kk][nn] = v;
+      rb[l] = v;
     }
-    __syncthreads();
+  };
+  auto store_tile = [&](int buf) {
+#pragma unroll
+    for (int l = 0; l < LA; ++l) {
+      const int e = tid + l * kGemmThreads;
+      if (FORM == kCN) As[buf][e / kBM][e % kBM] = ra[l];
+      else As[buf][e % BK][e / BK] = ra[l];
+    }
+#pragma unroll
+    for (int l = 0; l < LB; ++l) {
+      const int e = tid + l * kGemmThreads;
+      if (FORM == kNC) Bs[buf][e % BK][e / BK] = rb[l];
+      else Bs[buf][e / kBN][e % kBN] = rb[l];
+    }
+  };
+
+  int tile_count = 0, buf = 0;
+  if (kbeg < kend) {
+    load_tile(kbeg);
+    store_tile(0);
+  }
+  __syncthreads();
+  for (int k0 = kbeg; k0 < kend; k0 += BK) {
+    const bool more = k0 + BK < kend;
+    if (more) load_tile(k0 + BK);  // global loads in flight during the products below
 #pragma unroll
     for (int kk = 0; kk < BK; ++kk) {
       C a[4], b[4];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = As[kk][ty + 16 * i];
+      for (int i = 0; i < 4; ++i) a[i] = As[buf][kk][ty + 16 * i];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx + 16 * j];
+      for (int j = 0; j < 4; ++j) b[j] = Bs[buf][kk][tx + 16 * j];
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -111,7 +141,9 @@ cgemm_tile_kernel(Batch batch, int splits, cx_t<T> alpha, cx_t<T> beta, double2*
           acc[i][j].y += a[i].x * b[j].y + a[i].y * b[j].x;
         }
     }
+    if (more) store_tile(buf ^ 1);
     __syncthreads();
+    buf ^= 1;
     if constexpr (kFlush) {
       if (++tile_count == kFlushTiles) {
         tile_count = 0;

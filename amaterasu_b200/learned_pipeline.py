@@ -100,13 +100,14 @@ def run_cell(seed, pseudo, *, family="si8", ecut=15.0, density=None, precision="
     from .scf import run_scf
     structure, ref = make_cell(seed, family)
     system = build(structure, pseudo, family, ecut)
-    n0 = system.initial_density()
+    # timed: the start density (superposition or prediction) and the SCF
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    start = n0 if density is None else density(system)
+    start = system.initial_density() if density is None else density(system)
     res = run_scf(system, _config(family, precision), density=start)
     torch.cuda.synchronize()
     seconds = time.perf_counter() - t0
+    n0 = system.initial_density() if density is not None else start
     work = (FAMILIES[family]["grid"],) * 3
     return dict(seed=seed, grid=list(system.grid.shape), iterations=res.iterations, converged=res.converged,
                 free_energy=res.energies.free_energy, seconds=seconds,

@@ -13,7 +13,10 @@ Precision policy (``config.engine.precision``): "complex128" is the plain FP64 e
 complex128 once the density residual falls below ``refine_below``, or earlier when the
 complex64 iterations stop reducing it (best of the last ``stall_window`` iterations not
 below ``stall_ratio`` times the best before them: the FP32 rounding floor of a large cell
-can sit above ``refine_below``), so the fixed point is the FP64 one. Energies, densities, potentials and subspace eigensolves are FP64 always.
+can sit above ``refine_below``), so the fixed point is the FP64 one. The complex64
+Davidson tolerance is floored at ``c64_tolerance_floor``; ``refine_max_iterations`` > 0 caps
+the Davidson iterations per SCF step of the FP64 refinement (the orbitals are already
+converged to the FP32 floor; the SCF convergence test itself is unchanged). Energies, densities, potentials and subspace eigensolves are FP64 always.
 """
 from __future__ import annotations
 
@@ -217,6 +220,8 @@ def run_scf(system, config: Config | None = None, *, logger=None, wavefunctions=
         if orb.dtype == torch.complex64:
             tol = max(tol, config.engine.c64_tolerance_floor)  # FP32 residuals carry rounding noise
         maxit = 40 if iteration == 1 else 20
+        if policy == "mixed" and orb.dtype == torch.complex128 and config.engine.refine_max_iterations > 0:
+            maxit = config.engine.refine_max_iterations  # FP64 refinement of converged complex64 orbitals
         eigenvalues = np.empty((system.nspin, system.nkpoints, nb))
         for spin in range(system.nspin):
             if config.engine.batched:

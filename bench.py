@@ -33,6 +33,9 @@ REPO = Path(__file__).resolve().parent
 sys.path.insert(0, str(REPO))
 
 WORKLOAD = "si64_hpsi"
+# DRAM bytes of one complex64 all-k call, measured by ncu (sum over the call's kernels of
+# dram__bytes_read.sum + dram__bytes_write.sum on the one-k case, times 4 k-points)
+TRAFFIC_PER_CALL = 9.73e9
 METRIC = "Hpsi bands/s (Si64 40 Ry 84^3, 4 k x 160 bands)"
 
 
@@ -314,7 +317,10 @@ def main():
                    "kpoints": nk, "bands_per_k": nbands, "batched": "all k in one call",
                    "l2": "working set > L2 (no flush)", "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None,
+                     "frac": achieved / peak,
+                     "traffic": TRAFFIC_PER_CALL if (prec == "complex64" and nk == 4 and nbands == 160) else None,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the call's 7 kernels, "
+                                       "one-k capture x 4 (profiles/hpsi_si64_c64_kernels.md)",
                      "what": "whole H.psi call (stages A/B/C + projector GEMMs), algorithmic bytes",
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback"},
         "e2e": {"value": e2e_value, "unit": "bands/s",
