@@ -124,6 +124,30 @@ __device__ __forceinline__ void load_tw(C* dst, const C* src, int n) {
   for (int i = threadIdx.x; i < n; i += kFftThreads) dst[i] = src[i];
 }
 
+// Asynchronous global -> shared copy of n contiguous complex elements (cp.async): every
+// thread issues all of its copies before any completes, so a whole plane is in flight at
+// once. 16-byte copies when both ends are 16-byte aligned and the size is a multiple of 16,
+// else one copy per element. Completed by async_copy_wait().
+template <typename C>
+__device__ __forceinline__ void async_copy(C* dst, const C* src, int n) {
+  const uint32_t sdst = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
+  const size_t bytes = (size_t)n * sizeof(C);
+  if (((reinterpret_cast<uintptr_t>(src) | sdst) & 15) == 0 && (bytes & 15) == 0) {
+    const char* g = reinterpret_cast<const char*>(src);
+    for (int i = threadIdx.x; i < (int)(bytes >> 4); i += kFftThreads)
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sdst + 16 * i), "l"(g + 16 * i) : "memory");
+  } else {
+    for (int i = threadIdx.x; i < n; i += kFftThreads) {
+      if constexpr (sizeof(C) == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sdst + 16 * i), "l"(src + i) : "memory");
+      else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sdst + 8 * i), "l"(src + i) : "memory");
+    }
+  }
+}
+
+__device__ __forceinline__ void async_copy_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 template <typename T, class D>
 __global__ void __launch_bounds__(kFftThreads)
 stage_a_kernel(HpsiView v, const cx_t<T>* __restrict__ tw_y, const cx_t<T>* __restrict__ tw_z,
@@ -152,7 +176,19 @@ stage_a_kernel(HpsiView v, const cx_t<T>* __restrict__ tw_y, const cx_t<T>* __re
   __syncthreads();
   const int es = v.entry_start[k * (v.nslots + 1) + slot];
   const int ee = v.entry_start[k * (v.nslots + 1) + slot + 1];
-  for (int t = es + threadIdx.x; t < ee; t += kFftThreads) {
+  // scatter, four entries per thread in flight (the psi load depends on the entry load)
+  int t = es + threadIdx.x;
+  for (; t + 3 * kFftThreads < ee; t += 4 * kFftThreads) {
+    int2 en[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) en[u] = v.entries[t + u * kFftThreads];
+    C val[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) val[u] = src[en[u].x];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) pl[en[u].y] = val[u];
+  }
+  for (; t < ee; t += kFftThreads) {
     const int2 en = v.entries[t];
     pl[en.y] = src[en.x];
   }
@@ -309,20 +345,42 @@ stage_c_kernel(HpsiView v, const cx_t<T>* __restrict__ tw_y, const cx_t<T>* __re
   const int npw = v.npw[k];
   const int64_t boff = (v.pw_off[k] - v.pw_off[v.k_first]) * v.nbands + (int64_t)band * npw;
 
+  const C* srcw = work + (int64_t)gb * v.band_elems + (int64_t)slot * plane;
+  async_copy(pl, srcw, plane);  // the whole slot plane in flight while the tables load
   load_tw(sty, tw_y, n2);
   load_tw(stz, tw_z, n3);
-  const C* srcw = work + (int64_t)gb * v.band_elems + (int64_t)slot * plane;
-  for (int i = threadIdx.x; i < plane; i += kFftThreads) pl[i] = srcw[i];
   const int rs = v.row_start[k * (v.nslots + 1) + slot];
   const int nrows = v.row_start[k * (v.nslots + 1) + slot + 1] - rs;
   for (int i = threadIdx.x; i < nrows; i += kFftThreads) rows[i] = v.rows[rs + i];
+  async_copy_wait();
   __syncthreads();
   dft_cols<-1>(pl, n2, A2, B2, n3, sty);
   dft_rows<-1>(pl, n3, A3, B3, n3, rows, nrows, stz);
   const int es = v.entry_start[k * (v.nslots + 1) + slot];
   const int ee = v.entry_start[k * (v.nslots + 1) + slot + 1];
   const T* kk = kin + v.pw_off[k];
-  for (int t = es + threadIdx.x; t < ee; t += kFftThreads) {
+  // gather + T psi, four entries per thread in flight
+  int t = es + threadIdx.x;
+  for (; t + 3 * kFftThreads < ee; t += 4 * kFftThreads) {
+    int2 en[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) en[u] = v.entries[t + u * kFftThreads];
+    C p[4];
+    T tg[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      p[u] = psi[boff + en[u].x];
+      tg[u] = kk[en[u].x];
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      C r = pl[en[u].y];
+      r.x += tg[u] * p[u].x;
+      r.y += tg[u] * p[u].y;
+      hpsi[boff + en[u].x] = r;
+    }
+  }
+  for (; t < ee; t += kFftThreads) {
     const int2 en = v.entries[t];
     const C p = psi[boff + en.x];
     C r = pl[en.y];
