@@ -22,6 +22,7 @@
 #include "dft.cuh"
 #include "gemm.cuh"
 #include "engine_impl.cuh"
+#include "twiddles_line.h"
 
 #include <algorithm>
 #include <cmath>
@@ -252,6 +253,19 @@ stage_b_kernel(HpsiView v, const cx_t<T>* __restrict__ tw_xb, const cx_t<T>* __r
 // the same four-step DFTs as the shared-memory passes, done on a register array.
 constexpr int kRegBThreads = 128;
 
+// a * w^M with w = exp(S 2 pi i / N): an immediate twiddle when the line length has a
+// compile-time table, else a load from the uploaded table (which carries the sign)
+template <int N, int S, int M>
+__device__ __forceinline__ float2 line_twiddle(float2 a, const float2* __restrict__ tw) {
+  if constexpr (LineTwiddles<N>::kHave) {
+    constexpr float c = (float)LineTwiddles<N>::cos[M];
+    constexpr float s = (float)(S * LineTwiddles<N>::sin[M]);
+    return make_float2(a.x * c - a.y * s, a.x * s + a.y * c);
+  } else {
+    return cmul(a, __ldg(tw + M));
+  }
+}
+
 template <int N, int A, int S, bool NAT_IN>
 __device__ __forceinline__ void dft_line_reg(float2 (&v)[N], const float2* __restrict__ tw) {
   constexpr int B = N / A;
@@ -263,7 +277,7 @@ __device__ __forceinline__ void dft_line_reg(float2 (&v)[N], const float2* __res
       dft_reg<A, S>(t);
       static_for<A>([&](auto cc) {
         constexpr int c = decltype(cc)::value;
-        if constexpr (b * c % N != 0) t[c] = cmul(t[c], __ldg(tw + (b * c) % N));
+        if constexpr (b * c % N != 0) t[c] = line_twiddle<N, S, (b * c) % N>(t[c], tw);
         v[c * B + b] = t[c];
       });
     });
@@ -282,7 +296,7 @@ __device__ __forceinline__ void dft_line_reg(float2 (&v)[N], const float2* __res
       dft_reg<B, S>(t);
       static_for<B>([&](auto ee) {
         constexpr int e = decltype(ee)::value;
-        if constexpr (c * e % N != 0) t[e] = cmul(t[e], __ldg(tw + (c * e) % N));
+        if constexpr (c * e % N != 0) t[e] = line_twiddle<N, S, (c * e) % N>(t[e], tw);
         v[c * B + e] = t[e];
       });
     });
@@ -619,6 +633,25 @@ int hpsi_impl(AmaEngine* e, int k_first, int k_count, int nbands, int spin, cons
   const T* vpot = (p == AMA_C64 ? (const T*)e->d.v32 : (const T*)e->d.v64) + (int64_t)spin * e->N;
   const T* kin = p == AMA_C64 ? (const T*)e->d.kin32 : (const T*)e->d.kin64;
 
+  // complex64 tensor-core nonlocal path: the projection (split psi, P = psi B^H, reduce)
+  // reads only psi, so it runs on the engine's auxiliary stream while stages A-C run on s;
+  // s joins it before the apply, which adds into the stage C output
+  const bool tc_nl = e->nproj > 0 && std::is_same<T, float>::value && e->use_tc && e->tc.ready;
+  if (tc_nl) {
+    if (!e->aux) {
+      int lo = 0, hi = 0;
+      AMA_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+      AMA_CUDA_TRY(cudaStreamCreateWithPriority(&e->aux, cudaStreamNonBlocking, hi));
+      AMA_CUDA_TRY(cudaEventCreateWithFlags(&e->ev_in, cudaEventDisableTiming));
+      AMA_CUDA_TRY(cudaEventCreateWithFlags(&e->ev_nl, cudaEventDisableTiming));
+    }
+    AMA_CUDA_TRY(cudaEventRecord(e->ev_in, s));
+    AMA_CUDA_TRY(cudaStreamWaitEvent(e->aux, e->ev_in, 0));
+    rc = nl_tc_run(e, k_first, k_count, nbands, (const float2*)psi, (float2*)hpsi, e->aux, 0);
+    if (rc) return rc;
+    AMA_CUDA_TRY(cudaEventRecord(e->ev_nl, e->aux));
+  }
+
   rc = run_fft_stages_a<T>(e, v, (int)nb_total, psi, s);
   if (rc) return rc;
   if (e->regb[p]) {
@@ -637,8 +670,9 @@ int hpsi_impl(AmaEngine* e, int k_first, int k_count, int nbands, int spin, cons
       (const C*)e->work[p], (C*)hpsi);
   AMA_CHECK_LAUNCH();
 
-  if (e->nproj > 0 && std::is_same<T, float>::value && e->use_tc && e->tc.ready) {
-    rc = nl_tc_run(e, k_first, k_count, nbands, (const float2*)psi, (float2*)hpsi, s);
+  if (tc_nl) {
+    AMA_CUDA_TRY(cudaStreamWaitEvent(s, e->ev_nl, 0));
+    rc = nl_tc_run(e, k_first, k_count, nbands, (const float2*)psi, (float2*)hpsi, s, 1);
     if (rc) return rc;
   } else if (e->nproj > 0) {
     const size_t el = sizeof(C);
@@ -716,6 +750,11 @@ void free_grid_filters(const AmaEngine* e);
 void free_engine(AmaEngine* e) {
   free_grid_filters(e);
   nl_tc_free(e);
+  if (e->ev_in) cudaEventDestroy(e->ev_in);
+  if (e->ev_nl) cudaEventDestroy(e->ev_nl);
+  if (e->aux) cudaStreamDestroy(e->aux);
+  e->aux = nullptr;
+  e->ev_in = e->ev_nl = nullptr;
   auto f = [](void* p) { if (p) cudaFree(p); };
   f(e->d.plane_x); f(e->d.slot_of_x); f(e->d.entries); f(e->d.entry_start); f(e->d.rows);
   f(e->d.row_start); f(e->d.pw_off); f(e->d.npw); f(e->d.kin64); f(e->d.kin32); f(e->d.v64); f(e->d.v32);

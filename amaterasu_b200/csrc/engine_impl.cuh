@@ -76,12 +76,19 @@ struct AmaEngine {
   bool regb[2] = {false, false};    // [prec] stage B with register-resident x columns
   NlTcState tc;
   bool use_tc = true;
+  // the complex64 projection runs on this stream, concurrently with the FFT stages
+  cudaStream_t aux = nullptr;
+  cudaEvent_t ev_in = nullptr, ev_nl = nullptr;
 };
 
 namespace ama {
 int nl_tc_setup(AmaEngine* e);
+// phase 0: split psi, project, reduce (P -> split Q); phase 1: apply (hpsi += Q D B);
+// phase 2: both in order
 int nl_tc_run(AmaEngine* e, int k_first, int k_count, int nbands, const float2* psi, float2* hpsi,
-              cudaStream_t s);
+              cudaStream_t s, int phase = 2);
+int nl_tc_apply(AmaEngine* e, int k_first, int k_count, int nbands, float2* hpsi, cudaStream_t s, int ntile,
+                int bn);
 void nl_tc_free(AmaEngine* e);
 }  // namespace ama
 

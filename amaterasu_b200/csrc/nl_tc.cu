@@ -87,12 +87,18 @@ __global__ void split_psi_kernel(const float* __restrict__ psi, const int64_t* _
   const float* src = psi + 2 * ((pw_off[k] - pw_off[k_first]) * nbands + (int64_t)m * npw[k]);
   float* h = hi + ((int64_t)kl * nbp + m) * kp;
   float* l = lo + ((int64_t)kl * nbp + m) * kp;
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < kp; c += gridDim.x * blockDim.x) {
-    const float v = (m < nbands && c < np2) ? src[c] : 0.f;
-    float a, r;
-    tf32_split(v, a, r);
-    h[c] = a;
-    l[c] = r;
+  // four consecutive values per thread (kp is a multiple of 32, rows are 16-byte aligned)
+  for (int c = 4 * (blockIdx.x * blockDim.x + threadIdx.x); c < kp; c += 4 * gridDim.x * blockDim.x) {
+    float v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) v[u] = (m < nbands && c + u < np2) ? src[c + u] : 0.f;
+    float4 a, r;
+    tf32_split(v[0], a.x, r.x);
+    tf32_split(v[1], a.y, r.y);
+    tf32_split(v[2], a.z, r.z);
+    tf32_split(v[3], a.w, r.w);
+    *reinterpret_cast<float4*>(h + c) = a;
+    *reinterpret_cast<float4*>(l + c) = r;
   }
 }
 
@@ -197,11 +203,12 @@ int nl_tc_setup(AmaEngine* e) {
 }
 
 int nl_tc_run(AmaEngine* e, int k_first, int k_count, int nbands, const float2* psi, float2* hpsi,
-              cudaStream_t s) {
+              cudaStream_t s, int phase) {
   NlTcState& t = e->tc;
   const int ntile = (nbands + 255) / 256;
   const int bn = round_up((nbands + ntile - 1) / ntile, 16);
   const int nbp = bn * ntile;
+  if (phase == 1) return nl_tc_apply(e, k_first, k_count, nbands, hpsi, s, ntile, bn);
   // hi and lo halves live in one allocation each; maps are rebuilt whenever a buffer moves
   const size_t psi_half = (size_t)k_count * nbp * t.kp;
   const size_t q_half = (size_t)k_count * nbp * t.k2;
@@ -234,7 +241,7 @@ int nl_tc_run(AmaEngine* e, int k_first, int k_count, int nbands, const float2* 
     t.cached_nbp = nbp;
   }
 
-  dim3 gs((t.kp + 255) / 256, nbp, k_count);
+  dim3 gs((t.kp / 4 + 255) / 256, nbp, k_count);
   split_psi_kernel<<<gs, 256, 0, s>>>((const float*)psi, e->d.pw_off, e->d.npw, k_first, nbands, nbp, t.kp,
                                       t.psi[0], t.psi[1]);
   AMA_CHECK_LAUNCH();
@@ -257,7 +264,14 @@ int nl_tc_run(AmaEngine* e, int k_first, int k_count, int nbands, const float2* 
   dim3 gr(1, nbp, k_count);
   reduce_q_kernel<<<gr, 256, 0, s>>>(t.part, splits, nbp, t.p2, t.k2, e->nproj, t.q[0], t.q[1]);
   AMA_CHECK_LAUNCH();
+  if (phase == 0) return AMA_OK;
+  return nl_tc_apply(e, k_first, k_count, nbands, hpsi, s, ntile, bn);
+}
 
+// hpsi += P (D B) from the split Q of the projection phase
+int nl_tc_apply(AmaEngine* e, int k_first, int k_count, int nbands, float2* hpsi, cudaStream_t s, int ntile,
+                int bn) {
+  NlTcState& t = e->tc;
   ChainArgs b{};
   b.kblocks = t.k2 / kBK;
   b.splits = 1;
