@@ -112,6 +112,137 @@ __device__ __forceinline__ void dft_reg(C (&v)[R]) {
   }
 }
 
+// ------------------------------------------------------ sparse-input codelets
+// DFT of length R (sign S, natural order) whose inputs outside MASK (bit j set: v[j] may be
+// nonzero) are zero: the arithmetic on the zero inputs is skipped; the zero entries of v are
+// not read. Same transform as dft_reg, with the additions in the same order minus the zero
+// terms.
+template <int R, int S, uint32_t MASK, typename C>
+__device__ __forceinline__ void dft_reg_sparse(C (&v)[R]);
+
+template <int R, int S, uint32_t MASK, typename C>
+__device__ __forceinline__ void dft_odd_sparse(C (&v)[R]) {
+  using T = decltype(v[0].x);
+  constexpr int H = (R - 1) / 2;
+  constexpr bool in0 = (MASK & 1u) != 0;
+  C a[H + 1], b[H + 1];
+  static_for<H>([&](auto jj) {
+    constexpr int j = decltype(jj)::value + 1;
+    constexpr bool p = (MASK >> j) & 1u, q = (MASK >> (R - j)) & 1u;
+    if constexpr (p && q) {
+      a[j] = cadd(v[j], v[R - j]);
+      b[j] = csub(v[j], v[R - j]);
+    } else if constexpr (p) {
+      a[j] = v[j];
+      b[j] = v[j];
+    } else if constexpr (q) {
+      a[j] = v[R - j];
+      b[j] = mk<C>(-v[R - j].x, -v[R - j].y);
+    }
+  });
+  const C x0 = in0 ? v[0] : mk<C>(0, 0);
+  C sum = x0;
+  static_for<H>([&](auto jj) {
+    constexpr int j = decltype(jj)::value + 1;
+    if constexpr (((MASK >> j) & 1u) || ((MASK >> (R - j)) & 1u)) sum = cadd(sum, a[j]);
+  });
+  v[0] = sum;
+  static_for<H>([&](auto kk) {
+    constexpr int k = decltype(kk)::value + 1;
+    T ar = x0.x, ai = x0.y, br = T(0), bi = T(0);
+    static_for<H>([&](auto jj) {
+      constexpr int j = decltype(jj)::value + 1;
+      if constexpr (((MASK >> j) & 1u) || ((MASK >> (R - j)) & 1u)) {
+        constexpr int idx = (j * k) % R;
+        constexpr T c = (T)kCos[R][idx];
+        constexpr T s = (T)kSin[R][idx];
+        ar += a[j].x * c;
+        ai += a[j].y * c;
+        br += b[j].y * s;
+        bi += b[j].x * s;
+      }
+    });
+    if constexpr (S > 0) {
+      v[k].x = ar - br; v[k].y = ai + bi;
+      v[R - k].x = ar + br; v[R - k].y = ai - bi;
+    } else {
+      v[k].x = ar + br; v[k].y = ai - bi;
+      v[R - k].x = ar - br; v[R - k].y = ai + bi;
+    }
+  });
+}
+
+template <int M>
+constexpr uint32_t sparse_half_mask(uint32_t mask, int parity) {
+  uint32_t out = 0;
+  for (int i = 0; i < M; ++i)
+    if ((mask >> (2 * i + parity)) & 1u) out |= 1u << i;
+  return out;
+}
+
+template <int R, int S, uint32_t MASK, typename C>
+__device__ __forceinline__ void dft_even_sparse(C (&v)[R]) {
+  using T = decltype(v[0].x);
+  constexpr int M = R / 2;
+  constexpr uint32_t EM = sparse_half_mask<M>(MASK, 0), OM = sparse_half_mask<M>(MASK, 1);
+  C e[M], o[M];
+  static_for<M>([&](auto ii) {
+    constexpr int i = decltype(ii)::value;
+    if constexpr ((EM >> i) & 1u) e[i] = v[2 * i];
+    if constexpr ((OM >> i) & 1u) o[i] = v[2 * i + 1];
+  });
+  if constexpr (EM != 0) dft_reg_sparse<M, S, EM>(e);
+  if constexpr (OM != 0) dft_reg_sparse<M, S, OM>(o);
+  static_for<M>([&](auto kk) {
+    constexpr int k = decltype(kk)::value;
+    if constexpr (OM == 0) {
+      v[k] = e[k];
+      v[k + M] = e[k];
+    } else {
+      C t;
+      if constexpr (k == 0) {
+        t = o[k];
+      } else if constexpr (4 * k == R) {
+        t.x = -T(S) * o[k].y;
+        t.y = T(S) * o[k].x;
+      } else {
+        constexpr T c = (T)kCos[R][k];
+        constexpr T s = (T)(S * kSin[R][k]);
+        t.x = o[k].x * c - o[k].y * s;
+        t.y = o[k].x * s + o[k].y * c;
+      }
+      if constexpr (EM == 0) {
+        v[k] = t;
+        v[k + M] = mk<C>(-t.x, -t.y);
+      } else {
+        v[k] = cadd(e[k], t);
+        v[k + M] = csub(e[k], t);
+      }
+    }
+  });
+}
+
+template <int R, int S, uint32_t MASK, typename C>
+__device__ __forceinline__ void dft_reg_sparse(C (&v)[R]) {
+  constexpr uint32_t full = (R >= 32) ? 0xffffffffu : ((1u << R) - 1u);
+  if constexpr ((MASK & full) == full) {
+    dft_reg<R, S>(v);
+  } else if constexpr ((MASK & full) == 0) {
+    static_for<R>([&](auto kk) { v[decltype(kk)::value] = mk<C>(0, 0); });
+  } else if constexpr (R == 2) {
+    if constexpr (MASK & 1u) {
+      v[1] = v[0];
+    } else {
+      v[0] = v[1];
+      v[1] = mk<C>(-v[1].x, -v[1].y);
+    }
+  } else if constexpr (R % 2 == 0) {
+    dft_even_sparse<R, S, MASK>(v);
+  } else {
+    dft_odd_sparse<R, S, MASK>(v);
+  }
+}
+
 // ------------------------------------------------------------- smem passes
 // A "line" is n = A*B elements spaced `es` apart starting at `base`.
 //

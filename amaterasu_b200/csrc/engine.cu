@@ -339,6 +339,76 @@ stage_b_reg_kernel(HpsiView v, const float2* __restrict__ tw_xb, const float2* _
   });
 }
 
+// x-planes used by the spheres when they are the set x <= HP, x >= N - HN (Miller indices
+// -HN .. HP), numbered in increasing x
+template <int N, int HP, int HN>
+struct SlotSet {
+  static constexpr bool used(int x) { return x <= HP || x >= N - HN; }
+  static constexpr int slot(int x) { return x <= HP ? x : x - (N - HN - HP - 1); }
+  // inputs of the strided DFT-A at offset b (x = a B + b) that can be nonzero
+  static constexpr uint32_t line_mask(int A, int b) {
+    uint32_t m = 0;
+    for (int a = 0; a < A; ++a)
+      if (used(a * (N / A) + b)) m |= 1u << a;
+    return m;
+  }
+};
+
+// Stage B for a compile-time slot set: the x transform's zero inputs (x-planes without
+// sphere points) are skipped in the backward transform's first pass, and only the used
+// outputs of the forward transform are computed (the stores, and with them everything that
+// feeds only unused outputs, are resolved at compile time).
+template <int NX, int AX, int HP, int HN, class D>
+__global__ void __launch_bounds__(kRegBThreads)
+stage_b_sparse_kernel(HpsiView v, const float2* __restrict__ tw_xb, const float2* __restrict__ tw_xf,
+                      const float* __restrict__ vpot, float2* __restrict__ work) {
+  using SS = SlotSet<NX, HP, HN>;
+  constexpr int BX = NX / AX;
+  AMA_DIMS(D, v)
+  const int col = blockIdx.x * kRegBThreads + threadIdx.x;  // y * n3 + z
+  if (col >= plane) return;
+  float2* wb = work + (int64_t)blockIdx.y * v.band_elems + col;
+  float2 r[NX];
+  static_for<NX>([&](auto xx) {
+    constexpr int x = decltype(xx)::value;
+    if constexpr (SS::used(x)) r[x] = wb[(int64_t)SS::slot(x) * plane];
+  });
+  // backward x transform, natural in: strided DFT-A on the sparse inputs, twiddle, DFT-B
+  static_for<BX>([&](auto bb) {
+    constexpr int b = decltype(bb)::value;
+    constexpr uint32_t mask = SS::line_mask(AX, b);
+    float2 t[AX];
+    static_for<AX>([&](auto aa) {
+      constexpr int a = decltype(aa)::value;
+      if constexpr ((mask >> a) & 1u) t[a] = r[a * BX + b];
+    });
+    dft_reg_sparse<AX, +1, mask>(t);
+    static_for<AX>([&](auto cc) {
+      constexpr int c = decltype(cc)::value;
+      if constexpr (b * c % NX != 0) t[c] = line_twiddle<NX, +1, (b * c) % NX>(t[c], tw_xb);
+      r[c * BX + b] = t[c];
+    });
+  });
+  static_for<AX>([&](auto cc) {
+    constexpr int c = decltype(cc)::value;
+    float2 t[BX];
+    static_for<BX>([&](auto dd) { t[decltype(dd)::value] = r[c * BX + decltype(dd)::value]; });
+    dft_reg<BX, +1>(t);
+    static_for<BX>([&](auto dd) { r[c * BX + decltype(dd)::value] = t[decltype(dd)::value]; });
+  });
+  static_for<NX>([&](auto pp) {
+    constexpr int p = decltype(pp)::value;
+    const float s = __ldg(vpot + (int64_t)p * plane + col);
+    r[p].x *= s;
+    r[p].y *= s;
+  });
+  dft_line_reg<NX, AX, -1, false>(r, tw_xf);
+  static_for<NX>([&](auto xx) {
+    constexpr int x = decltype(xx)::value;
+    if constexpr (SS::used(x)) wb[(int64_t)SS::slot(x) * plane] = r[x];
+  });
+}
+
 template <typename T, class D>
 __global__ void __launch_bounds__(kFftThreads)
 stage_c_kernel(HpsiView v, const cx_t<T>* __restrict__ tw_y, const cx_t<T>* __restrict__ tw_z,
@@ -445,23 +515,29 @@ StageInfo fill_stage_table(const void** fn) {
 // (register-resident y columns for stages A and C were measured slower than the
 // shared-memory passes at 84^3 and are not used)
 template <int N1, int A1, int N2, int A2, int N3, class D>
-StageInfo fill_stage_table_reg(const void** fn) {
+StageInfo fill_stage_table_reg(const void** fn, int hp, int hn) {
   StageInfo info = fill_stage_table<float, D>(fn);
   fn[1] = (const void*)stage_b_reg_kernel<N1, A1, D>;
   info.regb = true;
+  if constexpr (N1 == 84) {  // the Si64 benchmark grid: sparse-x variants for its slot sets
+#define AMA_SPARSE(P, Q) \
+    if (hp == P && hn == Q) fn[1] = (const void*)stage_b_sparse_kernel<84, 12, P, Q, D>;
+    AMA_SPARSE(20, 20) AMA_SPARSE(20, 21) AMA_SPARSE(21, 20) AMA_SPARSE(21, 21)
+#undef AMA_SPARSE
+  }
   return info;
 }
 
 // Grids with compile-time kernels (cubic cells of the benchmark workloads); any other grid
 // runs the same kernels with sizes read at run time.
 template <typename T>
-StageInfo select_stage_table(const AxisPlan* ax, const void** fn) {
+StageInfo select_stage_table(const AxisPlan* ax, const void** fn, int hp, int hn) {
 #define AMA_FIX(N1, A1, N2, A2, N3, A3)                                                         \
   if (ax[0].n == N1 && ax[0].A == A1 && ax[1].n == N2 && ax[1].A == A2 && ax[2].n == N3 &&      \
       ax[2].A == A3) {                                                                           \
     using D = FixDims<N1, A1, N2, A2, N3, A3>;                                                   \
     if constexpr (std::is_same<T, float>::value && N1 <= 96)                                     \
-      return fill_stage_table_reg<N1, A1, N2, A2, N3, D>(fn);                                    \
+      return fill_stage_table_reg<N1, A1, N2, A2, N3, D>(fn, hp, hn);                            \
     else                                                                                         \
       return fill_stage_table<T, D>(fn);                                                         \
   }
@@ -584,7 +660,7 @@ int set_smem_limits(const AmaEngine* e) {
               "grid plane does not fit in shared memory at this precision");
   const int p = std::is_same<T, float>::value ? AMA_C64 : AMA_C128;
   const void** fn = const_cast<AmaEngine*>(e)->stage_fn[p];
-  const StageInfo info = select_stage_table<T>(e->ax, fn);
+  const StageInfo info = select_stage_table<T>(e->ax, fn, e->slot_hp, e->slot_hn);
   const_cast<AmaEngine*>(e)->zsplit[p] = info.zsplit;
   const_cast<AmaEngine*>(e)->regb[p] = info.regb;
   AMA_CUDA_TRY(cudaFuncSetAttribute(fn[0], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
@@ -819,6 +895,14 @@ extern "C" int ama_engine_create(const AmaSystemDesc* desc, AmaEngine** out) {
     if (x_used[x]) { slot_of_x[x] = (int)plane_x.size(); plane_x.push_back(x); }
   e->nslots = (int)plane_x.size();
   const int ns = e->nslots;
+  {  // is the slot set x <= hp, x >= n1 - hn (contiguous Miller range -hn .. hp)?
+    int hp = -1, hn = 0;
+    while (hp + 1 < n1 && x_used[hp + 1]) ++hp;
+    while (hn + 1 < n1 - hp - 1 && x_used[n1 - 1 - hn]) ++hn;
+    bool ok = hp >= 0;
+    for (int x = 0; x < n1 && ok; ++x) ok = (x_used[x] != 0) == (x <= hp || x >= n1 - hn);
+    if (ok) { e->slot_hp = hp; e->slot_hn = hn; }
+  }
 
   // per (k, slot): sphere entries and the y rows they occupy
   std::vector<int2> entries(total_pw);

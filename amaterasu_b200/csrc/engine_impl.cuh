@@ -55,6 +55,8 @@ struct AmaEngine {
   AxisPlan ax[3];
   int64_t N = 0;
   int nk = 0, nspin = 1, nproj = 0, nslots = 0;
+  // the used x-planes are exactly x <= slot_hp and x >= n1 - slot_hn (else both -1)
+  int slot_hp = -1, slot_hn = -1;
   uint32_t precisions = 0;
   std::vector<int> npw;
   std::vector<int64_t> pw_off;
