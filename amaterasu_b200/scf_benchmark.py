@@ -15,7 +15,8 @@ residual below 1e-7 per electron:
 
 Reported per run: SCF seconds (system set-up excluded, the same for every run),
 iterations, free energy, |dF| per atom against the plain run, and the largest force
-difference against the plain run (eV/A) when ``--forces`` is given.
+(eV/A) and stress (GPa) differences against the plain run when ``--forces`` / ``--stress``
+are given.
 """
 from __future__ import annotations
 
@@ -28,6 +29,7 @@ from pathlib import Path
 import numpy as np
 
 HARTREE_PER_BOHR_IN_EV_PER_ANG = 27.211386245988 / 0.529177210903
+HARTREE_PER_BOHR3_IN_GPA = 29421.015697
 SMEARING = {"si215_gamma": ("gaussian", "0.005 Ha"), "si8_batched": ("fermi-dirac", "0.01 Ha"),
             "si2_scf": ("fixed", None), "si64_hpsi": ("gaussian", "0.005 Ha")}
 
@@ -62,7 +64,7 @@ TRAINING_SPACING_A = 5.43 / 36  # working-grid spacing the committed nets were t
 
 
 def run(workload: str, weights=None, forces=False, log=print, policies=("plain", "mixed", "learned+mixed"),
-        engine_options=None, spacing=TRAINING_SPACING_A) -> dict:
+        engine_options=None, spacing=TRAINING_SPACING_A, stress=False) -> dict:
     import torch
     from .learned import DensityNet, LearnedStart, working_grid
     from .scf import run_scf
@@ -91,6 +93,9 @@ def run(workload: str, weights=None, forces=False, log=print, policies=("plain",
         if forces:
             from .properties import compute_forces
             row["_forces"] = compute_forces(system, res.density, res.wavefunctions, res.occupations)
+        if stress:
+            from .properties import compute_stress
+            row["_stress"] = compute_stress(system, res.density, res.wavefunctions, res.occupations)
         results[name] = row
         log(f"{name}: {seconds:.1f} s, {res.iterations} iterations, F = {res.energies.free_energy:.10f} Ha")
     plain = results.get("plain")
@@ -101,9 +106,13 @@ def run(workload: str, weights=None, forces=False, log=print, policies=("plain",
             if forces:
                 row["max_force_diff_eV_per_A"] = float(np.abs(row["_forces"] - plain["_forces"]).max()
                                                        * HARTREE_PER_BOHR_IN_EV_PER_ANG)
+            if stress:
+                row["max_stress_diff_GPa"] = float(np.abs(row["_stress"] - plain["_stress"]).max()
+                                                   * HARTREE_PER_BOHR3_IN_GPA)
         out["runs"][name] = row
     for row in results.values():
         row.pop("_forces", None)
+        row.pop("_stress", None)
     return out
 
 
@@ -126,6 +135,7 @@ def main():
     ap.add_argument("--workload", default="si215_gamma", choices=sorted(SMEARING))
     ap.add_argument("--weights", default=None)
     ap.add_argument("--forces", action="store_true")
+    ap.add_argument("--stress", action="store_true")
     ap.add_argument("--policies", default="plain,mixed,learned+mixed")
     ap.add_argument("--spacing", type=float, default=TRAINING_SPACING_A,
                     help="working-grid spacing (A) the network was trained at")
@@ -134,7 +144,7 @@ def main():
     ap.add_argument("--out", default=None)
     args = ap.parse_args()
     result = run(args.workload, args.weights, args.forces, policies=tuple(args.policies.split(",")),
-                 engine_options=parse_engine_options(args.engine), spacing=args.spacing)
+                 engine_options=parse_engine_options(args.engine), spacing=args.spacing, stress=args.stress)
     text = json.dumps(result, indent=1)
     print(text, flush=True)
     if args.out:
