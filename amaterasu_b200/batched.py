@@ -42,7 +42,8 @@ class _KOp:
 
 
 class BatchedDavidson:
-    def __init__(self, system, nbands: int, dtype=torch.complex128, tensor_cores: bool = True):
+    def __init__(self, system, nbands: int, dtype=torch.complex128, tensor_cores: bool = True,
+                 tc_min_npw: int = _TC_MIN_NPW):
         self.eng = engine_for(system)
         self.system = system
         self.nk = self.eng.nk
@@ -60,7 +61,7 @@ class BatchedDavidson:
         self.cap = self.max_sub + nbands
         # complex64 plane-wave products on the tensor cores (split-TF32) once the spheres are
         # long enough for the staged tiles to pay; shorter ones stay on the SIMT kernels
-        self.tensor_cores = bool(tensor_cores) and dtype == torch.complex64 and self.max_npw >= _TC_MIN_NPW
+        self.tensor_cores = bool(tensor_cores) and dtype == torch.complex64 and self.max_npw >= tc_min_npw
 
     # ---------------------------------------------------------------- kernels
     def _gemm(self, form, m, n, k, a: _KOp, b: _KOp, c: _KOp, alpha=1.0, beta=0.0, max_m=None, max_n=None):

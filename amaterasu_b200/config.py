@@ -66,6 +66,7 @@ class EngineConfig:
     stall_window: int = 3
     stall_ratio: float = 0.7
     tc_subspace: bool = True  # complex64 Davidson plane-wave products on the tensor cores
+    tc_min_npw: int = 8192    # ... for spheres of at least this many plane waves
     # lowest Davidson residual tolerance of the complex64 iterations: the FP32 H.psi and
     # subspace products leave a residual noise of a few 1e-7 Ha
     c64_tolerance_floor: float = 2e-6

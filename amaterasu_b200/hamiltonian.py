@@ -83,13 +83,16 @@ class Hamiltonian:
         return self.engine.hpsi(psi, out, k_first=k_first, k_count=k_count, nbands=nbands, spin=spin)
 
     def apply_host(self, host_in: torch.Tensor, host_out: torch.Tensor, nbands: int, spin: int = 0, *,
-                   dev_in: torch.Tensor | None = None, dev_out: torch.Tensor | None = None) -> None:
-        """Batched H.psi from host memory to host memory, pipelined over k-points.
+                   dev_in: torch.Tensor | None = None, dev_out: torch.Tensor | None = None,
+                   chunks_per_k: int = 1) -> None:
+        """Batched H.psi from host memory to host memory, pipelined over band chunks.
 
         ``host_in``/``host_out`` pack one (nbands, npw_k) block per k (pinned CPU tensors
-        for asynchronous copies). The copy of block k+1 in, the H.psi of block k and the copy
-        of block k-1 out overlap on three streams; the call returns with the work queued on
-        the current stream (synchronise before reading ``host_out``).
+        for asynchronous copies). Each k block is cut into ``chunks_per_k`` runs of bands; the
+        copy of chunk i+1 in, the H.psi of chunk i and the copy of chunk i-1 out overlap on
+        three streams, so only one chunk's copies are exposed at the start and the end. The
+        call returns with the work queued on the current stream (synchronise before reading
+        ``host_out``).
         """
         eng = self.engine
         offsets = eng.block_offsets(nbands)
@@ -107,15 +110,19 @@ class Hamiltonian:
         s_in.wait_stream(compute)
         s_out.wait_stream(compute)
         self._bind()
+        per = max(1, -(-nbands // max(1, int(chunks_per_k))))
         for k in range(eng.nk):
-            a, b = int(offsets[k]), int(offsets[k + 1])
-            with torch.cuda.stream(s_in):
-                dev_in[a:b].copy_(host_in[a:b], non_blocking=True)
-            compute.wait_stream(s_in)
-            eng.hpsi(dev_in[a:b], dev_out[a:b], k_first=k, k_count=1, nbands=nbands, spin=spin)
-            s_out.wait_stream(compute)
-            with torch.cuda.stream(s_out):
-                host_out[a:b].copy_(dev_out[a:b], non_blocking=True)
+            npw = int(eng.npw[k])
+            for r0 in range(0, nbands, per):
+                r1 = min(nbands, r0 + per)
+                a, b = int(offsets[k]) + r0 * npw, int(offsets[k]) + r1 * npw
+                with torch.cuda.stream(s_in):
+                    dev_in[a:b].copy_(host_in[a:b], non_blocking=True)
+                compute.wait_stream(s_in)
+                eng.hpsi(dev_in[a:b], dev_out[a:b], k_first=k, k_count=1, nbands=r1 - r0, spin=spin)
+                s_out.wait_stream(compute)
+                with torch.cuda.stream(s_out):
+                    host_out[a:b].copy_(dev_out[a:b], non_blocking=True)
         compute.wait_stream(s_out)
 
     def apply_overlap(self, coefficients, ik: int):

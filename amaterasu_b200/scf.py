@@ -229,7 +229,8 @@ def run_scf(system, config: Config | None = None, *, logger=None, wavefunctions=
                 key = ("_batched_davidson", orb.dtype)
                 bd = getattr(system, "_bd_cache", {}).get(key)
                 if bd is None:
-                    bd = BatchedDavidson(system, nb, orb.dtype, tensor_cores=config.engine.tc_subspace)
+                    bd = BatchedDavidson(system, nb, orb.dtype, tensor_cores=config.engine.tc_subspace,
+                                         tc_min_npw=config.engine.tc_min_npw)
                     system._bd_cache = {**getattr(system, "_bd_cache", {}), key: bd}
                 eps, X, _, _ = bd.run(H, orb.packed[spin], tolerance=tol, max_iterations=maxit, spin=spin)
                 eigenvalues[spin] = eps
