@@ -1,0 +1,74 @@
+"""Run-time choice of the H.psi kernel variants by timing them on the caller's shapes.
+
+The engine compiles several variants of the x-transform stage ("stage B": shared-memory
+slabs; register-resident x columns for short x lines; register-resident with the spheres'
+x-plane set fixed at compile time, for the benchmark grid) and two paths for the complex64
+nonlocal products (tcgen05 split-TF32 GEMMs or SIMT GEMMs). Which is fastest depends on the
+grid, the band count and the number of k-points of a call. ``autotune_hpsi`` times every
+available combination on the caller's Hamiltonian and block shape (CUDA events on the
+current stream after one warm-up call each), leaves the engine set to the fastest and
+returns the measurements; results are cached per (precision, nbands, k-point range) on the
+engine. All variants compute the same H.psi (``tests/test_autotune_gpu.py``).
+"""
+from __future__ import annotations
+
+import torch
+
+from .engine import TORCH_DTYPE, precision_code
+
+
+def _variants(eng, prec_code):
+    """Stage B variants the engine has for this precision (probe by selecting them)."""
+    out = []
+    for v in (0, 1, 2):
+        try:
+            eng.set_stage_b_variant(prec_code, v)
+            out.append(v)
+        except NotImplementedError:
+            pass
+    return out
+
+
+def autotune_hpsi(H, nbands: int, *, k_first: int = 0, k_count: int | None = None, reps: int = 3,
+                  force: bool = False) -> dict:
+    """Time the stage B variants x nonlocal paths for ``H.apply_all`` on blocks of ``nbands``
+    bands at k-points k_first .. k_first + k_count - 1, select the fastest on H's engine and
+    return ``{"stage_b": v, "nonlocal_tc": bool, "ms": {(v, tc): ms}}``."""
+    eng = H.engine
+    prec = precision_code(H.precision)
+    k_count = eng.nk - k_first if k_count is None else k_count
+    key = (prec, nbands, k_first, k_count)
+    cache = getattr(eng, "_autotune", None)
+    if cache is None:
+        cache = eng._autotune = {}
+    if key in cache and not force:
+        choice = cache[key]
+        eng.set_stage_b_variant(prec, choice["stage_b"])
+        eng.set_tensor_core_nonlocal(choice["nonlocal_tc"])
+        return choice
+    n = int(eng.pw_off[k_first + k_count] - eng.pw_off[k_first]) * nbands
+    g = torch.Generator(device=eng.device).manual_seed(7)
+    psi = torch.randn(n, dtype=TORCH_DTYPE[prec], device=eng.device, generator=g)
+    out = torch.empty_like(psi)
+    paths = [True, False] if (prec == 0 and eng.nproj > 0) else [True]
+    times = {}
+    stream = torch.cuda.current_stream(eng.device)
+    for v in _variants(eng, prec):
+        eng.set_stage_b_variant(prec, v)
+        for tc in paths:
+            eng.set_tensor_core_nonlocal(tc)
+            H.apply_all(psi, nbands, k_first=k_first, k_count=k_count, out=out)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                H.apply_all(psi, nbands, k_first=k_first, k_count=k_count, out=out)
+            e1.record(stream)
+            torch.cuda.synchronize(eng.device)
+            times[(v, tc)] = e0.elapsed_time(e1) / reps
+    best = min(times, key=times.get)
+    eng.set_stage_b_variant(prec, best[0])
+    eng.set_tensor_core_nonlocal(best[1])
+    choice = {"stage_b": best[0], "nonlocal_tc": best[1],
+              "ms": {f"stage_b={v},nonlocal_tc={int(tc)}": ms for (v, tc), ms in times.items()}}
+    cache[key] = choice
+    return choice

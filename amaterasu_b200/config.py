@@ -67,6 +67,7 @@ class EngineConfig:
     stall_ratio: float = 0.7
     tc_subspace: bool = True  # complex64 Davidson plane-wave products on the tensor cores
     tc_min_npw: int = 8192    # ... for spheres of at least this many plane waves
+    autotune: bool = True     # time the H.psi kernel variants once per precision and keep the fastest
     # lowest Davidson residual tolerance of the complex64 iterations: the FP32 H.psi and
     # subspace products leave a residual noise of a few 1e-7 Ha
     c64_tolerance_floor: float = 2e-6

@@ -500,7 +500,13 @@ density_b_kernel(HpsiView v, const cx_t<T>* __restrict__ tw_xb, const cx_t<T>* _
   }
 }
 
-struct StageInfo { int zsplit; bool regb; };
+// The stage B variants compiled for a grid: [0] shared-memory slab, [1] register-resident
+// x columns, [2] register-resident with the compile-time slot set (null when absent).
+struct StageInfo {
+  int zsplit;
+  bool regb;
+  const void* b_variant[3];
+};
 
 template <typename T, class D>
 StageInfo fill_stage_table(const void** fn) {
@@ -508,7 +514,7 @@ StageInfo fill_stage_table(const void** fn) {
   fn[1] = (const void*)stage_b_kernel<T, D>;
   fn[2] = (const void*)stage_c_kernel<T, D>;
   fn[3] = (const void*)density_b_kernel<T, D>;
-  return {D::zsplit, false};
+  return {D::zsplit, false, {fn[1], nullptr, nullptr}};
 }
 
 // complex64 on a compile-time grid with short x columns: register-resident stage B
@@ -519,9 +525,10 @@ StageInfo fill_stage_table_reg(const void** fn, int hp, int hn) {
   StageInfo info = fill_stage_table<float, D>(fn);
   fn[1] = (const void*)stage_b_reg_kernel<N1, A1, D>;
   info.regb = true;
+  info.b_variant[1] = fn[1];
   if constexpr (N1 == 84) {  // the Si64 benchmark grid: sparse-x variants for its slot sets
 #define AMA_SPARSE(P, Q) \
-    if (hp == P && hn == Q) fn[1] = (const void*)stage_b_sparse_kernel<84, 12, P, Q, D>;
+    if (hp == P && hn == Q) fn[1] = info.b_variant[2] = (const void*)stage_b_sparse_kernel<84, 12, P, Q, D>;
     AMA_SPARSE(20, 20) AMA_SPARSE(20, 21) AMA_SPARSE(21, 20) AMA_SPARSE(21, 21)
 #undef AMA_SPARSE
   }
@@ -663,10 +670,11 @@ int set_smem_limits(const AmaEngine* e) {
   const StageInfo info = select_stage_table<T>(e->ax, fn, e->slot_hp, e->slot_hn);
   const_cast<AmaEngine*>(e)->zsplit[p] = info.zsplit;
   const_cast<AmaEngine*>(e)->regb[p] = info.regb;
+  for (int i = 0; i < 3; ++i) const_cast<AmaEngine*>(e)->b_variant[p][i] = info.b_variant[i];
   AMA_CUDA_TRY(cudaFuncSetAttribute(fn[0], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
   AMA_CUDA_TRY(cudaFuncSetAttribute(fn[2], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
-  if (!info.regb)
-    AMA_CUDA_TRY(cudaFuncSetAttribute(fn[1], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)slab_b_smem<T>(e)));
+  AMA_CUDA_TRY(cudaFuncSetAttribute(info.b_variant[0], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)slab_b_smem<T>(e)));
   AMA_CUDA_TRY(cudaFuncSetAttribute(fn[3], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
   return AMA_OK;
 }
@@ -709,24 +717,11 @@ int hpsi_impl(AmaEngine* e, int k_first, int k_count, int nbands, int spin, cons
   const T* vpot = (p == AMA_C64 ? (const T*)e->d.v32 : (const T*)e->d.v64) + (int64_t)spin * e->N;
   const T* kin = p == AMA_C64 ? (const T*)e->d.kin32 : (const T*)e->d.kin64;
 
-  // complex64 tensor-core nonlocal path: the projection (split psi, P = psi B^H, reduce)
-  // reads only psi, so it runs on the engine's auxiliary stream while stages A-C run on s;
-  // s joins it before the apply, which adds into the stage C output
+  // complex64 tensor-core nonlocal path. Running its projection on a second stream next to
+  // the FFT stages was measured: ~1% faster on average, but with the projection's
+  // 222 KB-shared-memory CTAs waiting for whole SMs to drain, some runs were 50% slower, so
+  // the products run in stream order after stage C.
   const bool tc_nl = e->nproj > 0 && std::is_same<T, float>::value && e->use_tc && e->tc.ready;
-  if (tc_nl) {
-    if (!e->aux) {
-      int lo = 0, hi = 0;
-      AMA_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&lo, &hi));
-      AMA_CUDA_TRY(cudaStreamCreateWithPriority(&e->aux, cudaStreamNonBlocking, hi));
-      AMA_CUDA_TRY(cudaEventCreateWithFlags(&e->ev_in, cudaEventDisableTiming));
-      AMA_CUDA_TRY(cudaEventCreateWithFlags(&e->ev_nl, cudaEventDisableTiming));
-    }
-    AMA_CUDA_TRY(cudaEventRecord(e->ev_in, s));
-    AMA_CUDA_TRY(cudaStreamWaitEvent(e->aux, e->ev_in, 0));
-    rc = nl_tc_run(e, k_first, k_count, nbands, (const float2*)psi, (float2*)hpsi, e->aux, 0);
-    if (rc) return rc;
-    AMA_CUDA_TRY(cudaEventRecord(e->ev_nl, e->aux));
-  }
 
   rc = run_fft_stages_a<T>(e, v, (int)nb_total, psi, s);
   if (rc) return rc;
@@ -747,8 +742,7 @@ int hpsi_impl(AmaEngine* e, int k_first, int k_count, int nbands, int spin, cons
   AMA_CHECK_LAUNCH();
 
   if (tc_nl) {
-    AMA_CUDA_TRY(cudaStreamWaitEvent(s, e->ev_nl, 0));
-    rc = nl_tc_run(e, k_first, k_count, nbands, (const float2*)psi, (float2*)hpsi, s, 1);
+    rc = nl_tc_run(e, k_first, k_count, nbands, (const float2*)psi, (float2*)hpsi, s);
     if (rc) return rc;
   } else if (e->nproj > 0) {
     const size_t el = sizeof(C);
@@ -826,11 +820,6 @@ void free_grid_filters(const AmaEngine* e);
 void free_engine(AmaEngine* e) {
   free_grid_filters(e);
   nl_tc_free(e);
-  if (e->ev_in) cudaEventDestroy(e->ev_in);
-  if (e->ev_nl) cudaEventDestroy(e->ev_nl);
-  if (e->aux) cudaStreamDestroy(e->aux);
-  e->aux = nullptr;
-  e->ev_in = e->ev_nl = nullptr;
   auto f = [](void* p) { if (p) cudaFree(p); };
   f(e->d.plane_x); f(e->d.slot_of_x); f(e->d.entries); f(e->d.entry_start); f(e->d.rows);
   f(e->d.row_start); f(e->d.pw_off); f(e->d.npw); f(e->d.kin64); f(e->d.kin32); f(e->d.v64); f(e->d.v32);
@@ -1352,6 +1341,17 @@ extern "C" int ama_engine_option(AmaEngine* e, int32_t option, int32_t value) {
     case 0:  // nonlocal products of the complex64 path on the tensor cores (1) or SIMT (0)
       e->use_tc = value != 0;
       return AMA_OK;
+    case 1:  // complex64 stage B variant: 0 shared memory, 1 register, 2 register + slot set
+    case 2: {  // complex128 stage B variant (only 0 is compiled)
+      const int p = option == 1 ? AMA_C64 : AMA_C128;
+      AMA_REQUIRE(e->precisions & (1u << p), AMA_ERR_ARG, "the engine was created without this precision");
+      AMA_REQUIRE(value >= 0 && value < 3, AMA_ERR_ARG, "stage B variant must be 0, 1 or 2");
+      AMA_REQUIRE(e->b_variant[p][value] != nullptr, AMA_ERR_UNSUPPORTED,
+                  "this stage B variant is not compiled for the engine's grid");
+      e->stage_fn[p][1] = e->b_variant[p][value];
+      e->regb[p] = value != 0;
+      return AMA_OK;
+    }
     default:
       ama::set_error("unknown engine option");
       return AMA_ERR_ARG;

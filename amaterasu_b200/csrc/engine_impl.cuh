@@ -76,11 +76,9 @@ struct AmaEngine {
   const void* stage_fn[2][4] = {};  // [prec][stage A, B, C, density B] (grid-specialised)
   int zsplit[2] = {1, 1};           // [prec] z halves per stage-B slab
   bool regb[2] = {false, false};    // [prec] stage B with register-resident x columns
+  const void* b_variant[2][3] = {};  // [prec] stage B variants compiled for the grid
   NlTcState tc;
   bool use_tc = true;
-  // the complex64 projection runs on this stream, concurrently with the FFT stages
-  cudaStream_t aux = nullptr;
-  cudaEvent_t ev_in = nullptr, ev_nl = nullptr;
 };
 
 namespace ama {

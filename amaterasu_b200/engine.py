@@ -105,6 +105,13 @@ class DeviceEngine:
         or to the SIMT GEMM."""
         call("ama_engine_option", self.handle, 0, 1 if enabled else 0)
 
+    def set_stage_b_variant(self, precision, variant: int) -> None:
+        """Select the stage B kernel (x transforms and V): 0 shared-memory slabs, 1 register-
+        resident x columns, 2 register-resident with the compile-time x-plane set. Raises
+        NotImplementedError when the variant is not compiled for this grid."""
+        option = 1 if precision_code(precision) == AMA_C64 else 2
+        call("ama_engine_option", self.handle, option, int(variant))
+
     def tc_status(self) -> int:
         code = ct.c_int32(0)
         call("ama_tc_status", self.handle, ct.byref(code))

@@ -26,6 +26,7 @@ from dataclasses import dataclass, field
 import numpy as np
 import torch
 
+from .autotune import autotune_hpsi
 from .batched import BatchedDavidson
 from .config import Config, parse_energy
 from .density import accumulate_packed, band_weights, finalize_density
@@ -216,6 +217,8 @@ def run_scf(system, config: Config | None = None, *, logger=None, wavefunctions=
         trace.append(prec_name)
         veff, _, _ = effective_potential(system, rho_in)
         H = Hamiltonian(system, veff, precision=prec_name)
+        if config.engine.autotune:  # kernel variants timed once per precision on this system
+            autotune_hpsi(H, nb)
         tol = float(np.clip(1e-3 * min(residual, 1.0), 1e-11, 1e-6))
         if orb.dtype == torch.complex64:
             tol = max(tol, config.engine.c64_tolerance_floor)  # FP32 residuals carry rounding noise

@@ -42,13 +42,14 @@ METRIC = "Hpsi bands/s (Si64 40 Ry 84^3, 4 k x 160 bands)"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["complex64", "complex128"], default="complex64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--kpoints", type=int, default=4, help="k-points of the workload to include (profiling)")
     ap.add_argument("--no-extras", action="store_true", help="skip the e2e and complex128 legs (profiling)")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the engine's default kernel variants")
     ap.add_argument("--scf", action="store_true",
                     help="also time the Si215 Gamma SCF (plain FP64, mixed, learned+mixed; several minutes)")
     return ap.parse_args()
@@ -91,42 +92,63 @@ def algorithmic_bytes(system, nbands, itemsize):
 
 
 class ClockSampler:
+    """SM clock and throttle reasons during the timed region: one `nvidia-smi -lms 200`
+    process started (and seen to answer) before the region, stopped after it. A fresh
+    nvidia-smi per sample initialises NVML each time, which was seen to stall the GPU for
+    tens of milliseconds inside short timed regions."""
+
     def __init__(self, index):
         self.index = index
-        self.samples = []
-        self._stop = threading.Event()
+        self.lines = []
+        self._proc = None
         self._t = None
 
-    def start(self):
-        def run():
-            q = ("--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
-                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-                 "clocks_event_reasons.sw_power_cap")
-            while not self._stop.is_set():
-                try:
-                    out = subprocess.run(["nvidia-smi", q, "--format=csv,noheader,nounits", "-i",
-                                          str(self.index)], capture_output=True, text=True, timeout=5)
-                    self.samples.append([x.strip() for x in out.stdout.strip().split(",")])
-                except Exception:
-                    pass
-                self._stop.wait(0.2)
-        self._t = threading.Thread(target=run, daemon=True)
-        self._t.start()
+    def start(self, wait_s: float = 5.0):
+        q = ("--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self._proc = subprocess.Popen(["nvidia-smi", q, "--format=csv,noheader,nounits", "-i", str(self.index),
+                                           "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                                          text=True)
+        except Exception:
+            self._proc = None
+            return
 
-    def stop(self):
-        self._stop.set()
+        def reader():
+            for line in self._proc.stdout:
+                self.lines.append([x.strip() for x in line.strip().split(",")])
+        self._t = threading.Thread(target=reader, daemon=True)
+        self._t.start()
+        t0 = time.time()
+        while not self.lines and time.time() - t0 < wait_s and self._proc.poll() is None:
+            time.sleep(0.05)
+
+    def mark(self):
+        """Index of the next sample (samples from here on are inside the timed region)."""
+        return len(self.lines)
+
+    def stop(self, first: int = 0):
+        if self._proc is not None:
+            time.sleep(0.25)  # at least one sample after the region
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=5)
+            except Exception:
+                self._proc.kill()
         if self._t:
-            self._t.join(timeout=10)
-        if not self.samples:
+            self._t.join(timeout=5)
+        samples = self.lines[max(0, first - 1):] or self.lines
+        if not samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[0]) for s in self.samples if len(s) >= 6 and s[0].replace(".", "").isdigit()]
-        mx = [float(s[1]) for s in self.samples if len(s) >= 6 and s[1].replace(".", "").isdigit()]
+        sm = [float(s[0]) for s in samples if len(s) >= 6 and s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in samples if len(s) >= 6 and s[1].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples if len(s) >= 6
+        reasons = sorted({names[i] for s in samples if len(s) >= 6
                           for i in range(4) if s[2 + i].strip() == "Active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
-                "samples": len(self.samples)}
+                "samples": len(samples)}
 
 
 def cpu_hpsi_sample(system, veff, nbands_sample, seconds, threads):
@@ -228,6 +250,10 @@ def main():
     eng.reserve(prec, nk * nbands)
     stream = torch.cuda.current_stream()
 
+    # kernel variants chosen by timing them on this workload (amaterasu_b200.autotune)
+    from amaterasu_b200.autotune import autotune_hpsi
+    tuned = {"stage_b": "default", "nonlocal_tc": True} if args.no_autotune else autotune_hpsi(H, nbands)
+
     def step():
         H.apply_all(psi, nbands, out=out)
 
@@ -237,6 +263,7 @@ def main():
 
     sampler = ClockSampler(local)
     sampler.start()
+    first_sample = sampler.mark()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -265,7 +292,7 @@ def main():
         e1.record(stream)
         torch.cuda.synchronize()
         e2e_ms = e0.elapsed_time(e1)
-    clocks = sampler.stop()
+    clocks = sampler.stop(first_sample)
 
     t = torch.tensor([ms, e2e_ms], dtype=torch.float64, device="cuda")
     if world > 1:
@@ -315,7 +342,8 @@ def main():
                    "ecut_ry": 40, "grid": list(system.grid.shape),
                    "npw": [len(w) for w in system.wave_spheres], "nproj": len(system.projectors[0]),
                    "kpoints": nk, "bands_per_k": nbands, "batched": "all k in one call",
-                   "l2": "working set > L2 (no flush)", "parallelism": f"replicas x{world}"},
+                   "l2": "working set > L2 (no flush)", "parallelism": f"replicas x{world}",
+                   "autotune": {"stage_b": tuned["stage_b"], "nonlocal_tc": tuned["nonlocal_tc"]}},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak,
                      "traffic": TRAFFIC_PER_CALL if (prec == "complex64" and nk == 4 and nbands == 160) else None,
@@ -325,7 +353,9 @@ def main():
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback"},
         "e2e": {"value": e2e_value, "unit": "bands/s",
                 "h2d_bytes_per_step": int(host.nbytes), "d2h_bytes_per_step": int(host.nbytes)},
-        "gpu_launches": args.steps * (7 if prec == "complex64" else 6),
+        # per call: stages A, B, C + (complex64, tensor cores) psi split, project, reduce, apply
+        # or (SIMT) project, its split-K reduce, apply
+        "gpu_launches": args.steps * (7 if (prec == "complex64" and tuned["nonlocal_tc"]) else 6),
         "clocks": clocks,
         **extra,
     }

@@ -66,8 +66,14 @@ AMA_API int ama_version(void);
 AMA_API int ama_engine_create(const AmaSystemDesc* desc, AmaEngine** engine);
 AMA_API int ama_engine_destroy(AmaEngine* engine);
 
-/* Engine options: option 0 = nonlocal products of the complex64 path on the tensor cores
- * (value 1, default) or on the SIMT GEMM (value 0). No counterpart in the reference. */
+/* Engine options (no counterpart in the reference):
+ *   option 0: nonlocal products of the complex64 path on the tensor cores (value 1, default)
+ *             or on the SIMT GEMM (value 0);
+ *   option 1: complex64 stage B (x transforms and V) variant: 0 shared-memory slabs,
+ *             1 register-resident x columns, 2 register-resident with the spheres' compile-time
+ *             x-plane set; AMA_ERR_UNSUPPORTED when the variant is not compiled for the grid;
+ *   option 2: the same for complex128 (only variant 0 exists).
+ * amaterasu_b200.autotune times the variants and keeps the fastest. */
 AMA_API int ama_engine_option(AmaEngine* engine, int32_t option, int32_t value);
 
 /* Device-side status of the tensor-core kernels (0 = fine; otherwise the code of the
