@@ -190,6 +190,163 @@ cgemm_tile_kernel(Batch batch, int splits, cx_t<T> alpha, cx_t<T> beta, double2*
   }
 }
 
+// FP64 complex GEMM on the FP64 tensor cores (mma.sync m8n8k4, DMMA): same forms, batches,
+// split-K and epilogue as cgemm_tile_kernel<double>. A CTA computes a 64 x 64 complex tile
+// with 8 warps (2 along M x 4 along N), each warp 32 x 16 complex = 4 x 2 blocks of 8 x 8.
+// The k-tile (8) is staged as separate real and imaginary planes, k-major with a 72-double
+// row pitch (the fragment loads of a warp then take the minimum two wavefronts), double
+// buffered with a register prefetch of the next tile. Per 8 x 8 block and k-step of 4:
+//   Re C += Ar Br + (-Ai) Bi,   Im C += Ar Bi + Ai Br   (four DMMAs).
+constexpr int kDmmaBK = 8;
+constexpr int kDmmaPitch = kBM + 8;
+
+__device__ __forceinline__ void dmma_884(double (&c)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(c[0]), "+d"(c[1])
+               : "d"(a), "d"(b));
+}
+
+template <int FORM, class Batch>
+__global__ void __launch_bounds__(kGemmThreads)
+zgemm_dmma_kernel(Batch batch, int splits, double2 alpha, double2 beta, double2* partial, int64_t partial_stride) {
+  using C = double2;
+  constexpr int BK = kDmmaBK, P = kDmmaPitch;
+  constexpr int LA = BK * kBM / kGemmThreads, LB = BK * kBN / kGemmThreads;  // 2 and 2
+  __shared__ double Ar[2][BK][P], Ai[2][BK][P], Br[2][BK][P], Bi[2][BK][P];
+
+  const int z = blockIdx.z;
+  const int bz = z / splits, sz = z % splits;
+  const GemmProblem<C> p = batch(bz);
+  const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * kBN;
+  if (m0 >= p.m || n0 >= p.n) return;
+  const int kchunk = ((p.k + splits - 1) / splits + BK - 1) / BK * BK;
+  const int kbeg = sz * kchunk;
+  const int kend = min(p.k, kbeg + kchunk);
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = (warp & 1) * 32, wn = (warp >> 1) * 16;
+  const int fr = lane >> 2, fk = lane & 3;  // fragment row (m or n) and k of this lane
+
+  double cre[4][2][2], cim[4][2][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j) cre[i][j][0] = cre[i][j][1] = cim[i][j][0] = cim[i][j][1] = 0.0;
+
+  C ra[LA], rb[LB];
+  auto load_tile = [&](int k0) {
+#pragma unroll
+    for (int l = 0; l < LA; ++l) {
+      const int e = tid + l * kGemmThreads;
+      int mm, kk;
+      if (FORM == kCN) { mm = e % kBM; kk = e / kBM; }
+      else { kk = e % BK; mm = e / BK; }
+      const int gm = m0 + mm, gk = k0 + kk;
+      C v = make_double2(0.0, 0.0);
+      if (gm < p.m && gk < kend) {
+        if (FORM == kCN) { v = p.a[(int64_t)gk * p.lda + gm]; v.y = -v.y; }
+        else v = p.a[(int64_t)gm * p.lda + gk];
+      }
+      ra[l] = v;
+    }
+#pragma unroll
+    for (int l = 0; l < LB; ++l) {
+      const int e = tid + l * kGemmThreads;
+      int nn, kk;
+      if (FORM == kNC) { kk = e % BK; nn = e / BK; }
+      else { nn = e % kBN; kk = e / kBN; }
+      const int gn = n0 + nn, gk = k0 + kk;
+      C v = make_double2(0.0, 0.0);
+      if (gn < p.n && gk < kend) {
+        if (FORM == kNC) { v = p.b[(int64_t)gn * p.ldb + gk]; v.y = -v.y; }
+        else v = p.b[(int64_t)gk * p.ldb + gn];
+      }
+      rb[l] = v;
+    }
+  };
+  auto store_tile = [&](int buf) {
+#pragma unroll
+    for (int l = 0; l < LA; ++l) {
+      const int e = tid + l * kGemmThreads;
+      int mm, kk;
+      if (FORM == kCN) { mm = e % kBM; kk = e / kBM; }
+      else { kk = e % BK; mm = e / BK; }
+      Ar[buf][kk][mm] = ra[l].x;
+      Ai[buf][kk][mm] = ra[l].y;
+    }
+#pragma unroll
+    for (int l = 0; l < LB; ++l) {
+      const int e = tid + l * kGemmThreads;
+      int nn, kk;
+      if (FORM == kNC) { kk = e % BK; nn = e / BK; }
+      else { nn = e % kBN; kk = e / kBN; }
+      Br[buf][kk][nn] = rb[l].x;
+      Bi[buf][kk][nn] = rb[l].y;
+    }
+  };
+
+  int buf = 0;
+  if (kbeg < kend) {
+    load_tile(kbeg);
+    store_tile(0);
+  }
+  __syncthreads();
+  for (int k0 = kbeg; k0 < kend; k0 += BK) {
+    const bool more = k0 + BK < kend;
+    if (more) load_tile(k0 + BK);
+#pragma unroll
+    for (int ks = 0; ks < BK; ks += 4) {
+      double ar[4], ai[4], nai[4], br[2], bi[2];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        ar[i] = Ar[buf][ks + fk][wm + 8 * i + fr];
+        ai[i] = Ai[buf][ks + fk][wm + 8 * i + fr];
+        nai[i] = -ai[i];
+      }
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        br[j] = Br[buf][ks + fk][wn + 8 * j + fr];
+        bi[j] = Bi[buf][ks + fk][wn + 8 * j + fr];
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          dmma_884(cre[i][j], ar[i], br[j]);
+          dmma_884(cre[i][j], nai[i], bi[j]);
+          dmma_884(cim[i][j], ar[i], bi[j]);
+          dmma_884(cim[i][j], ai[i], br[j]);
+        }
+    }
+    if (more) store_tile(buf ^ 1);
+    __syncthreads();
+    buf ^= 1;
+  }
+
+  // lane holds C[wm + 8 i + fr][wn + 8 j + 2 fk + t]
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int gm = m0 + wm + 8 * i + fr;
+    if (gm >= p.m) continue;
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int t = 0; t < 2; ++t) {
+        const int gn = n0 + wn + 8 * j + 2 * fk + t;
+        if (gn >= p.n) continue;
+        const C sum = make_double2(cre[i][j][t], cim[i][j][t]);
+        if (partial) {
+          partial[(int64_t)z * partial_stride + (int64_t)gm * p.n + gn] = sum;
+        } else {
+          C* dst = p.c + (int64_t)gm * p.ldc + gn;
+          C r = cmul(alpha, sum);
+          if (beta.x != 0.0 || beta.y != 0.0) r = cadd(r, cmul(beta, *dst));
+          *dst = r;
+        }
+      }
+  }
+}
+
 // Sum the split-K partials of each batch and apply the epilogue.
 template <typename T, class Batch>
 __global__ void cgemm_reduce_kernel(Batch batch, int splits, cx_t<T> alpha, cx_t<T> beta,
@@ -222,12 +379,18 @@ cudaError_t launch_cgemm(Batch batch, int nbatch, int max_m, int max_n, int spli
                          cx_t<T> alpha, cx_t<T> beta, double2* partial, int64_t partial_stride,
                          cudaStream_t stream) {
   dim3 grid((max_n + kBN - 1) / kBN, (max_m + kBM - 1) / kBM, nbatch * splits);
-  if (splits <= 1) {
-    cgemm_tile_kernel<T, FORM><<<grid, kGemmThreads, 0, stream>>>(batch, 1, alpha, beta, nullptr, 0);
-    return cudaGetLastError();
+  if constexpr (std::is_same<T, double>::value) {  // FP64: the FP64 tensor cores
+    zgemm_dmma_kernel<FORM><<<grid, kGemmThreads, 0, stream>>>(batch, splits <= 1 ? 1 : splits, alpha, beta,
+                                                               splits <= 1 ? nullptr : partial, partial_stride);
+    if (splits <= 1) return cudaGetLastError();
+  } else {
+    if (splits <= 1) {
+      cgemm_tile_kernel<T, FORM><<<grid, kGemmThreads, 0, stream>>>(batch, 1, alpha, beta, nullptr, 0);
+      return cudaGetLastError();
+    }
+    cgemm_tile_kernel<T, FORM><<<grid, kGemmThreads, 0, stream>>>(batch, splits, alpha, beta, partial,
+                                                                  partial_stride);
   }
-  cgemm_tile_kernel<T, FORM><<<grid, kGemmThreads, 0, stream>>>(batch, splits, alpha, beta, partial,
-                                                                partial_stride);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   dim3 rgrid(64, nbatch);
