@@ -90,13 +90,16 @@ class BatchedDavidson:
         g = g.to(torch.complex128)
         return 0.5 * (g + g.conj().transpose(1, 2))
 
-    def _heev(self, mats: torch.Tensor):
-        """Batched FP64 Hermitian eigensolve: (w ascending [nk][n], V columns [nk][n][n])."""
+    def _heev(self, mats: torch.Tensor, lowest: int | None = None):
+        """Batched FP64 Hermitian eigensolve: (w ascending [nk][n], V columns [nk][n][n]).
+        With ``lowest``, only the first ``lowest`` eigenpairs are valid (large n only)."""
         n = mats.shape[1]
         m = mats.contiguous().clone()
         w = torch.empty((self.nk, n), dtype=torch.float64, device=self.dev)
         if n <= _JACOBI_MAX:
             call("ama_heev_small", n, ptr(m), ptr(w), self.nk, stream_ptr())
+        elif lowest is not None and lowest < n:
+            call("ama_heev_lowest", n, int(lowest), ptr(m), ptr(w), self.nk, stream_ptr())
         else:
             call("ama_heev", n, ptr(m), ptr(w), self.nk, stream_ptr())
         return w, m
@@ -140,7 +143,7 @@ class BatchedDavidson:
         p = p * (~inval)[:, :, None] * (~inval)[:, None, :]
         bound = p.abs().sum(dim=2).max(dim=1, keepdim=True).values + _GAP  # per-k Gershgorin bound
         p = p + torch.diag_embed(inval.to(torch.float64) * bound).to(torch.complex128)
-        w, v = self._heev(p)
+        w, v = self._heev(p, lowest=self.nb)  # only the nb lowest Ritz pairs are kept
         rot = v[:, :, :self.nb].transpose(1, 2)  # (nb x m) per k: X_n = sum_i V[i, n] b_i
         X = self._rotate(rot, B, self.cap, m, self.nb)
         HX = self._rotate(rot, HB, self.cap, m, self.nb)

@@ -86,6 +86,59 @@ extern "C" int ama_heev(int32_t n, void* matrices, double* eigenvalues, int32_t 
   return AMA_OK;
 }
 
+// The lowest nvec eigenpairs only (zheevdx, index range 1..nvec): the tridiagonal reduction
+// is the same, but bisection and inverse iteration replace divide and conquer and only nvec
+// vectors are back-transformed. Eigenvalues [0, nvec) ascending; eigenvectors in columns
+// [0, nvec) (row-major, as ama_heev); the other entries are undefined.
+extern "C" int ama_heev_lowest(int32_t n, int32_t nvec, void* matrices, double* eigenvalues, int32_t batch,
+                               void* stream) {
+  AMA_REQUIRE(matrices && eigenvalues, AMA_ERR_ARG, "null argument");
+  AMA_REQUIRE(n >= 1 && batch >= 1 && nvec >= 1 && nvec <= n, AMA_ERR_SHAPE, "bad sizes");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!g_solver.handle) {
+    if (cusolverDnCreate(&g_solver.handle) != CUSOLVER_STATUS_SUCCESS) {
+      set_error("cusolverDnCreate failed");
+      return AMA_ERR_CUDA;
+    }
+    AMA_CUDA_TRY(cudaMalloc((void**)&g_solver.info, 2 * sizeof(int)));
+  }
+  cusolverDnSetStream(g_solver.handle, s);
+  int lwork = 0, meig = 0;
+  if (cusolverDnZheevdx_bufferSize(g_solver.handle, CUSOLVER_EIG_MODE_VECTOR, CUSOLVER_EIG_RANGE_I,
+                                   CUBLAS_FILL_MODE_LOWER, n, (cuDoubleComplex*)matrices, n, 0.0, 0.0, 1, nvec,
+                                   &meig, eigenvalues, &lwork) != CUSOLVER_STATUS_SUCCESS) {
+    set_error("cusolverDnZheevdx_bufferSize failed");
+    return AMA_ERR_CUDA;
+  }
+  const size_t need = (size_t)lwork * sizeof(cuDoubleComplex);
+  if (g_solver.work_bytes < need) {
+    if (g_solver.work) cudaFree(g_solver.work);
+    g_solver.work = nullptr; g_solver.work_bytes = 0;
+    AMA_CUDA_TRY(cudaMalloc(&g_solver.work, need));
+    g_solver.work_bytes = need;
+  }
+  AMA_CUDA_TRY(cudaMemsetAsync(g_solver.info + 1, 0, sizeof(int), s));
+  for (int b = 0; b < batch; ++b) {
+    cuDoubleComplex* a = (cuDoubleComplex*)matrices + (int64_t)b * n * n;
+    if (cusolverDnZheevdx(g_solver.handle, CUSOLVER_EIG_MODE_VECTOR, CUSOLVER_EIG_RANGE_I, CUBLAS_FILL_MODE_LOWER,
+                          n, a, n, 0.0, 0.0, 1, nvec, &meig, eigenvalues + (int64_t)b * n,
+                          (cuDoubleComplex*)g_solver.work, lwork, g_solver.info) != CUSOLVER_STATUS_SUCCESS) {
+      set_error("cusolverDnZheevdx failed");
+      return AMA_ERR_CUDA;
+    }
+    check_info_kernel<<<1, 32, 0, s>>>(g_solver.info, g_solver.info + 1);
+  }
+  dim3 grid(std::max(1, std::min(64, (n * n + 255) / 256)), batch);
+  conj_transpose_kernel<<<grid, 256, 0, s>>>((double2*)matrices, n);
+  AMA_CHECK_LAUNCH();
+  int flag = 0;
+  AMA_CUDA_TRY(cudaMemcpyAsync(&flag, g_solver.info + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+  AMA_CUDA_TRY(cudaStreamSynchronize(s));
+  AMA_REQUIRE(flag == 0, AMA_ERR_NOT_CONVERGED, "zheevdx did not converge");
+  AMA_REQUIRE(meig == nvec, AMA_ERR_NOT_CONVERGED, "zheevdx returned fewer eigenpairs than asked for");
+  return AMA_OK;
+}
+
 namespace {
 // Keep only the row-major upper triangle (where the column-major lower result lands),
 // then conjugate-transpose so the row-major lower triangle holds the result.

@@ -222,6 +222,14 @@ AMA_API int ama_lda_pz(const double* rho, int64_t npoints, double* eps, double* 
  * Replaces scipy.linalg.eigh in rayleigh_ritz (scf/eigen/subspace.py:74). */
 AMA_API int ama_heev(int32_t n, void* matrices, double* eigenvalues, int32_t batch, void* stream);
 
+/* The lowest nvec eigenpairs of each matrix (as ama_heev: eigenvalues ascending in
+ * eigenvalues[b*n + 0 .. nvec), eigenvectors in row-major columns 0 .. nvec-1; the rest of
+ * both is undefined). Bisection and inverse iteration on the tridiagonal form (zheevdx):
+ * the Rayleigh-Ritz step needs only the nbands lowest of m = up to 5 nbands Ritz pairs
+ * (subspace.py:74 computes all of them with scipy.linalg.eigh). */
+AMA_API int ama_heev_lowest(int32_t n, int32_t nvec, void* matrices, double* eigenvalues, int32_t batch,
+                            void* stream);
+
 /* The same for many small matrices (order n <= 80) at once: one CTA per matrix, cyclic
  * Jacobi in shared memory, FP64. Used for the per-k-point Rayleigh-Ritz problems of the
  * batched Davidson (scf/eigen/subspace.py:74 for every k). */

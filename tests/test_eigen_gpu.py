@@ -129,3 +129,26 @@ def test_batched_davidson_matches_per_k(mini_system, dtype, tol):
         blk = X[off:off + s.nbands * len(w)].reshape(s.nbands, len(w)).to(torch.complex128).cpu().numpy()
         off += s.nbands * len(w)
         np.testing.assert_allclose(blk @ blk.conj().T, np.eye(s.nbands), atol=1e-5 if dtype == torch.complex64 else 1e-11)
+
+
+@pytest.mark.parametrize("n,nvec", [(120, 24), (300, 60), (97, 97)])
+def test_heev_lowest_matches_eigh(n, nvec):
+    """ama_heev_lowest (zheevdx, index range) against numpy's eigh: the nvec lowest
+    eigenvalues, orthonormal eigenvectors and their residuals, on a batch of two."""
+    from amaterasu_b200._lib import call
+    from amaterasu_b200.engine import ptr, stream_ptr
+    rng = np.random.default_rng(n + nvec)
+    batch = 2
+    a = rng.normal(size=(batch, n, n)) + 1j * rng.normal(size=(batch, n, n))
+    a = a + np.conj(np.transpose(a, (0, 2, 1)))
+    m = torch.from_numpy(a.copy()).cuda()
+    w = torch.empty((batch, n), dtype=torch.float64, device="cuda")
+    call("ama_heev_lowest", n, nvec, ptr(m), ptr(w), batch, stream_ptr())
+    w = w.cpu().numpy()[:, :nvec]
+    v = m.cpu().numpy()[:, :, :nvec]
+    for b in range(batch):
+        ref = np.linalg.eigvalsh(a[b])[:nvec]
+        scale = max(1.0, np.abs(ref).max())
+        np.testing.assert_allclose(w[b], ref, rtol=0, atol=1e-11 * scale)
+        np.testing.assert_allclose(v[b].conj().T @ v[b], np.eye(nvec), atol=1e-10)
+        np.testing.assert_allclose(a[b] @ v[b], v[b] * w[b][None, :], atol=1e-9 * scale)
