@@ -295,3 +295,40 @@ extern "C" int ama_kbatch_copy_rows(int32_t precision, int32_t nk, int32_t nrows
   AMA_CHECK_LAUNCH();
   return AMA_OK;
 }
+
+// ---------------------------------------------------------------- structure sums
+// out[g] = scale * sum_a radial[species[a]][g] * exp(-i G_g . tau_a): the superposition of
+// per-species radial form factors with the atoms' phases (reference hamiltonian/local.py:
+// 37-74, structure factors and per-species sums). One thread per G vector, looping over
+// the atoms in FP64 (sincos of G.tau).
+namespace {
+__global__ void structure_sum_kernel(const double* __restrict__ gcart, int ng, const double* __restrict__ pos,
+                                     const int* __restrict__ species, int natoms, const double* __restrict__ radial,
+                                     double scale, double2* __restrict__ out) {
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ng; g += gridDim.x * blockDim.x) {
+    const double gx = gcart[3 * g], gy = gcart[3 * g + 1], gz = gcart[3 * g + 2];
+    double re = 0.0, im = 0.0;
+    for (int a = 0; a < natoms; ++a) {
+      const double th = gx * __ldg(pos + 3 * a) + gy * __ldg(pos + 3 * a + 1) + gz * __ldg(pos + 3 * a + 2);
+      double s, c;
+      sincos(th, &s, &c);
+      const double f = __ldg(radial + (int64_t)__ldg(species + a) * ng + g);
+      re += f * c;
+      im -= f * s;
+    }
+    out[g] = make_double2(scale * re, scale * im);
+  }
+}
+}  // namespace
+
+extern "C" int ama_structure_sum(const double* gcart, int32_t ng, const double* positions, const int32_t* species,
+                                 int32_t natoms, const double* radial, double scale, double* out, void* stream) {
+  AMA_REQUIRE(gcart && positions && species && radial && out, AMA_ERR_ARG, "null argument");
+  AMA_REQUIRE(ng >= 0 && natoms >= 0, AMA_ERR_SHAPE, "negative size");
+  if (ng == 0) return AMA_OK;
+  const int blocks = std::max(1, std::min(4 * 148, (ng + 255) / 256));
+  structure_sum_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(gcart, ng, positions, species, natoms, radial,
+                                                                 scale, (double2*)out);
+  AMA_CHECK_LAUNCH();
+  return AMA_OK;
+}

@@ -3,7 +3,9 @@
 Restates amaterasu ``hamiltonian/local.py``: per-species radial transforms on the density
 sphere combined with phases ``e^{-iG.tau}``, divided by Omega, scattered to the grid and
 transformed with no 1/N (:37-74); the valence density is floored at 1e-12 and rescaled
-to the electron count (:77-106). These run once per geometry on the host in FP64.
+to the electron count (:77-106). These run once per geometry in FP64: the structure sums on
+the GPU (ama_structure_sum) when one is present, else on the host; the transform to the
+grid on the host.
 """
 from __future__ import annotations
 
@@ -24,12 +26,42 @@ def _to_real_grid(grid, sphere, coefficients) -> np.ndarray:
     return _sfft.ifftn(field, norm="forward")
 
 
+def _device_structure_sum(sphere, positions, symbols, radial, scale):
+    """sum_a radial[symbol_a](G) exp(-i G.tau_a) * scale through ama_structure_sum when a
+    CUDA device is present (the atoms x G phase matrix of the host form is ~2 GB and
+    seconds of exp() at 215 atoms and 30 Ry); None without one."""
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return None
+        import ctypes as ct
+
+        from ._lib import call, load
+        load()
+    except Exception:
+        return None
+    names = sorted(radial)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    g = torch.from_numpy(np.ascontiguousarray(sphere.cartesian, dtype=np.float64)).to(dev)
+    pos = torch.from_numpy(np.ascontiguousarray(np.atleast_2d(positions), dtype=np.float64)).to(dev)
+    spc = torch.tensor([names.index(s) for s in symbols], dtype=torch.int32, device=dev)
+    rad = torch.from_numpy(np.ascontiguousarray(np.stack([np.asarray(radial[s], float) for s in names]))).to(dev)
+    out = torch.empty(len(sphere), dtype=torch.complex128, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    call("ama_structure_sum", ct.c_void_p(g.data_ptr()), len(sphere), ct.c_void_p(pos.data_ptr()),
+         ct.c_void_p(spc.data_ptr()), len(symbols), ct.c_void_p(rad.data_ptr()), float(scale),
+         ct.c_void_p(out.data_ptr()), ct.c_void_p(stream.cuda_stream))
+    return out.cpu().numpy()
+
+
 def _superpose(grid, sphere, positions, symbols, radial) -> np.ndarray:
-    phases = structure_factors(sphere, positions)
-    coefficients = np.zeros(len(sphere), dtype=complex)
-    for atom, symbol in enumerate(symbols):
-        coefficients += radial[symbol] * phases[atom]
-    coefficients /= grid.volume
+    coefficients = _device_structure_sum(sphere, positions, symbols, radial, 1.0 / grid.volume)
+    if coefficients is None:  # host form (CPU-only set-up, tests)
+        phases = structure_factors(sphere, positions)
+        coefficients = np.zeros(len(sphere), dtype=complex)
+        for atom, symbol in enumerate(symbols):
+            coefficients += radial[symbol] * phases[atom]
+        coefficients /= grid.volume
     return _to_real_grid(grid, sphere, coefficients)
 
 

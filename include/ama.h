@@ -217,6 +217,14 @@ AMA_API int ama_kbatch_copy_rows(int32_t precision, int32_t nk, int32_t nrows, c
  * Replaces lda.exchange + lda.correlation_pz81 (xc/lda.py:122-142,203-262). */
 AMA_API int ama_lda_pz(const double* rho, int64_t npoints, double* eps, double* vrho, void* stream);
 
+/* Structure sums of the set-up (superposed atomic densities and local potentials):
+ *   out[g] = scale * sum_a radial[species[a] * ng + g] * exp(-i G_g . tau_a)
+ * gcart: device FP64 [ng][3] Cartesian G vectors; positions: [natoms][3] Bohr; species:
+ * int32 [natoms] row of `radial` (device FP64 [nspecies][ng]); out: complex128 [ng].
+ * Replaces the phase matrix and per-atom sums of hamiltonian/local.py:37-74. */
+AMA_API int ama_structure_sum(const double* gcart, int32_t ng, const double* positions, const int32_t* species,
+                              int32_t natoms, const double* radial, double scale, double* out, void* stream);
+
 /* Dense FP64 Hermitian eigensolver for `batch` matrices of order n (device, row-major,
  * interleaved complex, overwritten by eigenvectors as columns); eigenvalues ascending.
  * Replaces scipy.linalg.eigh in rayleigh_ritz (scf/eigen/subspace.py:74). */
