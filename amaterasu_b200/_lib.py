@@ -76,6 +76,7 @@ SIGNATURES = {
     "ama_grid_filter_noalloc": (ct.c_int, [_P, _I32, _I32, _P, _P, _P, _P]),
     "ama_heev": (ct.c_int, [_I32, _P, _P, _I32, _P]),
     "ama_heev_lowest": (ct.c_int, [_I32, _I32, _P, _P, _I32, _P]),
+    "ama_solver_status": (ct.c_int, [ct.POINTER(ct.c_int32)]),
     "ama_structure_sum": (ct.c_int, [_P, _I32, _P, _P, _I32, _P, ct.c_double, _P, _P]),
     "ama_potrf_inv": (ct.c_int, [_I32, _P, _I32, _P]),
     "ama_heev_small": (ct.c_int, [_I32, _P, _P, _I32, _P]),

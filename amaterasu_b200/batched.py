@@ -14,8 +14,10 @@ active bands, or directions dropped as dependent), its surplus rows are zero and
 invalid: their Rayleigh-Ritz diagonal is set just above that k's Gershgorin bound of the
 valid block, which decouples them without inflating the matrix norm (the Jacobi solver's
 stopping rule is relative to it).
-Orthonormalisation (initial block and new directions) uses the Gram eigendecomposition,
-which spans the same space as the reference's Cholesky/SVD, so the Ritz pairs agree.
+Orthonormalisation: the initial block and the rank-revealing pass over the new directions
+use the Gram eigendecomposition, which spans the same space as the reference's SVD; the
+second pass (the reference's Cholesky) is a Newton-Schulz symmetric orthonormalisation on
+FP64 GEMMs, the overlap being the identity to within rounding there. The Ritz pairs agree.
 """
 from __future__ import annotations
 
@@ -133,6 +135,47 @@ class BatchedDavidson:
         out = self._rotate(rot, blk, rows, rows, rows)
         return out, keep.cpu().numpy()
 
+    def _small_gemm(self, a, b, out, rows):
+        """out[k] = a[k] b[k] for the nk small (rows x rows) complex128 matrices (FP64 tensor cores)."""
+        one = (ct.c_double * 2)(1.0, 0.0)
+        zero = (ct.c_double * 2)(0.0, 0.0)
+        st = rows * rows
+        call("ama_zgemm", AMA_C128, 0, rows, rows, rows, one, ptr(a), rows, st, ptr(b), rows, st, zero, ptr(out),
+             rows, st, self.nk, stream_ptr())
+        return out
+
+    def _lowdin_rows(self, blk: torch.Tensor, rows: int, keep: np.ndarray):
+        """Rows of each k's block re-orthonormalised by the Newton-Schulz iteration for
+        S^{-1/2} (S = the rows' overlap, coupled form Y <- Y T, Z <- T Z, T = (3I - Z Y)/2):
+        a symmetric (Loewdin) orthonormalisation on FP64 GEMMs, for rows that are already
+        orthonormal to within rounding (the second pass after the rank-revealing one).
+        Invalid (zero) rows are decoupled and stay zero. Returns None when the overlap is too
+        far from the identity for the iteration (the caller then decomposes it)."""
+        g = self._gram(blk, rows, rows)
+        inval = torch.from_numpy(~keep[:, :rows]).to(self.dev)
+        eye = torch.eye(rows, dtype=torch.complex128, device=self.dev).expand(self.nk, rows, rows)
+        g = g * (~inval)[:, :, None] * (~inval)[:, None, :] + torch.diag_embed(inval.to(torch.complex128))
+        dev = float(torch.linalg.matrix_norm(g - eye).max())  # Frobenius, >= spectral norm
+        if not dev < 0.5:
+            return None
+        iters = 0
+        err = max(dev, 1e-300)
+        while err > 1e-18 and iters < 6:
+            err *= err
+            iters += 1
+        y = g.contiguous()
+        z = eye.contiguous().clone()
+        t = torch.empty_like(y)
+        tmp = torch.empty_like(y)
+        for _ in range(iters):
+            self._small_gemm(z, y, t, rows)
+            t = 1.5 * eye - 0.5 * t
+            self._small_gemm(y, t, tmp, rows)
+            y, tmp = tmp, y
+            self._small_gemm(t, z, tmp, rows)
+            z, tmp = tmp, z
+        return self._rotate(z, blk, rows, rows, rows)
+
     def _rr(self, B, HB, m, valid):
         p = self._small(m, m)
         self._gemm(1, m, m, -1, _KOp(B, self.cap, 0), _KOp(HB, self.cap, 0),
@@ -160,9 +203,14 @@ class BatchedDavidson:
         block per k; returns (eigenvalues [nk][nb] numpy, X packed, norms numpy, iterations)."""
         nb, cap = self.nb, self.cap
         H._bind()
-        X0, ok = self._orthonormal_rows(guess_packed.to(self.dtype).contiguous(), nb, 1e-10, False)
-        if not ok.all():
-            raise ValueError("the starting block of some k-point is rank deficient")
+        guess = guess_packed.to(self.dtype).contiguous()
+        # the guess is usually the previous step's orthonormal orbitals: polish them without a
+        # decomposition, else decompose the overlap (and reject a rank-deficient start)
+        X0 = self._lowdin_rows(guess, nb, np.ones((self.nk, nb), dtype=bool))
+        if X0 is None:
+            X0, ok = self._orthonormal_rows(guess, nb, 1e-10, False)
+            if not ok.all():
+                raise ValueError("the starting block of some k-point is rank deficient")
         B, HB = self._blocks(cap), self._blocks(cap)
         HX0 = self._apply(H, X0, nb, spin)
         self._copy(X0, nb, 0, B, cap, 0, nb)
@@ -199,7 +247,11 @@ class BatchedDavidson:
             new, keep1 = self._orthonormal_rows(C, nn, 1e-7, True)
             if not keep1.any():
                 break
-            new, keep = self._orthonormal_rows(new, nn, 0.5, False)
+            polished = self._lowdin_rows(new, nn, keep1)
+            if polished is not None:
+                new, keep = polished, keep1
+            else:
+                new, keep = self._orthonormal_rows(new, nn, 0.5, False)
             HN = self._apply(H, new, nn, spin)
             self._copy(new, nn, 0, B, cap, m, nn)
             self._copy(HN, nn, 0, HB, cap, m, nn)

@@ -13,7 +13,7 @@ HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 LIB = HERE / "libama.so"
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
-SOURCES = ["api.cu", "engine.cu", "nl_tc.cu", "subspace_tc.cu", "gemm_api.cu", "vecops.cu", "eig.cu", "convnet.cu"]
+SOURCES = ["api.cu", "engine.cu", "nl_tc.cu", "subspace_tc.cu", "gemm_api.cu", "vecops.cu", "eig.cu", "hermitian.cu", "convnet.cu"]
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
     "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
@@ -54,7 +54,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         raise RuntimeError("nvcc failed:\n" + "\n".join(failed))
     tmp = LIB.with_suffix(".so.tmp")
     link = [NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objects, "-o", str(tmp),
-            "-L/usr/local/cuda/lib64", "-lcusolver", "-Xlinker", "-rpath=/usr/local/cuda/lib64"]
+            "-L/usr/local/cuda/lib64", "-Xlinker", "-rpath=/usr/local/cuda/lib64"]
     subprocess.run(link, check=True)
     os.replace(tmp, LIB)
     return LIB

@@ -43,6 +43,23 @@ template <int N, class F> __device__ __forceinline__ void static_for(F&& f) {
 // Thread-local last-error message for the C-ABI.
 void set_error(const std::string& msg);
 
+// Library state that holds device memory is kept per CUDA device: a process that drives
+// several GPUs must never hand one device's buffer to a kernel on another.
+constexpr int kMaxDevices = 64;
+inline int current_device() {
+  int d = 0;
+  if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= kMaxDevices) return -1;
+  return d;
+}
+template <typename T> struct PerDevice {
+  T slot[kMaxDevices];
+  // The current device's instance, or nullptr when the device id is unusable.
+  T* here() {
+    const int d = current_device();
+    return d < 0 ? nullptr : &slot[d];
+  }
+};
+
 }  // namespace ama
 
 #define AMA_CUDA_TRY(expr)                                                              \

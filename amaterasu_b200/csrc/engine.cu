@@ -26,6 +26,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <atomic>
 #include <map>
 #include <numeric>
 #include <vector>
@@ -815,7 +816,7 @@ int upload_twiddles(AmaEngine* e, int prec) {
   return AMA_OK;
 }
 
-void free_grid_filters(const AmaEngine* e);
+void free_grid_filters(AmaEngine* e);
 
 void free_engine(AmaEngine* e) {
   free_grid_filters(e);
@@ -844,6 +845,11 @@ extern "C" int ama_engine_create(const AmaSystemDesc* desc, AmaEngine** out) {
               "projectors and dij are required when nproj > 0");
   AMA_REQUIRE((desc->precisions & 3u) != 0, AMA_ERR_ARG, "no precision requested");
   AmaEngine* e = new AmaEngine();
+  if (cudaGetDevice(&e->device) != cudaSuccess) {
+    delete e;
+    ama::set_error("ama_engine_create: no current CUDA device");
+    return AMA_ERR_CUDA;
+  }
   const int dims[3] = {desc->n1, desc->n2, desc->n3};
   for (int a = 0; a < 3; ++a) {
     if (dims[a] < 1 || !split_length(dims[a], &e->ax[a])) {
@@ -994,6 +1000,10 @@ extern "C" int ama_engine_create(const AmaSystemDesc* desc, AmaEngine** out) {
   if (e->nproj > 0 && (e->precisions & (1u << AMA_C64))) {
     rc = nl_tc_setup(e);
     if (rc) { free_engine(e); return rc; }
+  }
+  if (int rc = ama::noalloc_prepare()) {  // the fixed grid array's address, before any capture
+    free_engine(e);
+    return rc;
   }
   *out = e;
   return AMA_OK;
@@ -1239,20 +1249,38 @@ __global__ void __launch_bounds__(kFftThreads) grid_g2f_kernel(GridView g, const
 }
 }  // namespace
 
-struct AmaGridFilters {
-  double* filt[4] = {};
-};
-static std::map<const AmaEngine*, AmaGridFilters> g_filters;
 namespace {
-void free_grid_filters(const AmaEngine* e) {
-  auto it = g_filters.find(e);
-  if (it == g_filters.end()) return;
-  for (double* p : it->second.filt) if (p) cudaFree(p);
-  g_filters.erase(it);
+void free_grid_filters(AmaEngine* e) {
+  for (double*& p : e->grid_filt) {
+    if (p) cudaFree(p);
+    p = nullptr;
+  }
+  if (e->grid_work) cudaFree(e->grid_work);
+  e->grid_work = nullptr;
+  e->grid_work_bytes = 0;
+}
+
+int ensure_grid_work(AmaEngine* e) {
+  const size_t need = (size_t)e->N * sizeof(double2);
+  if (e->grid_work_bytes >= need) return AMA_OK;
+  if (e->grid_work) cudaFree(e->grid_work);
+  e->grid_work = nullptr;
+  e->grid_work_bytes = 0;
+  AMA_CUDA_TRY(cudaMalloc((void**)&e->grid_work, need));
+  e->grid_work_bytes = need;
+  return AMA_OK;
+}
+
+// The engine's tables live on the device that was current at ama_engine_create.
+int require_engine_device(const AmaEngine* e) {
+  int dev = 0;
+  AMA_CUDA_TRY(cudaGetDevice(&dev));
+  AMA_REQUIRE(dev == e->device, AMA_ERR_ARG,
+              "the engine was created on device " + std::to_string(e->device) + " but device " +
+                  std::to_string(dev) + " is current");
+  return AMA_OK;
 }
 }  // namespace
-static double2* g_grid_work = nullptr;
-static size_t g_grid_work_bytes = 0;
 
 extern "C" int ama_set_grid_filter(AmaEngine* e, int32_t slot, const double* filter) {
   AMA_REQUIRE(e && filter, AMA_ERR_ARG, "null argument");
@@ -1270,9 +1298,9 @@ extern "C" int ama_set_grid_filter(AmaEngine* e, int32_t slot, const double* fil
       }
     }
   }
-  AmaGridFilters& f = g_filters[e];
-  if (!f.filt[slot]) AMA_CUDA_TRY(cudaMalloc((void**)&f.filt[slot], (size_t)e->N * sizeof(double)));
-  AMA_CUDA_TRY(cudaMemcpy(f.filt[slot], perm.data(), (size_t)e->N * sizeof(double), cudaMemcpyHostToDevice));
+  if (int rc = require_engine_device(e)) return rc;
+  if (!e->grid_filt[slot]) AMA_CUDA_TRY(cudaMalloc((void**)&e->grid_filt[slot], (size_t)e->N * sizeof(double)));
+  AMA_CUDA_TRY(cudaMemcpy(e->grid_filt[slot], perm.data(), (size_t)e->N * sizeof(double), cudaMemcpyHostToDevice));
   return AMA_OK;
 }
 
@@ -1280,21 +1308,15 @@ extern "C" int ama_grid_filter(AmaEngine* e, int32_t slot, int32_t energy_slot, 
                                double* out, double* energy, void* stream) {
   AMA_REQUIRE(e && in && out, AMA_ERR_ARG, "null argument");
   AMA_REQUIRE(slot >= 0 && slot < 4 && energy_slot >= -1 && energy_slot < 4, AMA_ERR_ARG, "bad slot");
-  auto it = g_filters.find(e);
-  AMA_REQUIRE(it != g_filters.end() && it->second.filt[slot], AMA_ERR_ARG, "filter slot not set");
+  AMA_REQUIRE(e->grid_filt[slot], AMA_ERR_ARG, "filter slot not set");
   const double* ef = nullptr;
   if (energy_slot >= 0) {
-    ef = it->second.filt[energy_slot];
+    ef = e->grid_filt[energy_slot];
     AMA_REQUIRE(ef && energy, AMA_ERR_ARG, "energy filter slot not set or energy is null");
   }
+  if (int rc = require_engine_device(e)) return rc;
   cudaStream_t s = (cudaStream_t)stream;
-  const size_t need = (size_t)e->N * sizeof(double2);
-  if (g_grid_work_bytes < need) {
-    if (g_grid_work) cudaFree(g_grid_work);
-    g_grid_work = nullptr; g_grid_work_bytes = 0;
-    AMA_CUDA_TRY(cudaMalloc((void**)&g_grid_work, need));
-    g_grid_work_bytes = need;
-  }
+  if (int rc = ensure_grid_work(e)) return rc;
   GridView g = grid_view(e);
   const size_t ps = plane_smem<double>(e), ss = slab_smem<double>(e);
   AMA_CUDA_TRY(cudaFuncSetAttribute(grid_g1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
@@ -1302,12 +1324,12 @@ extern "C" int ama_grid_filter(AmaEngine* e, int32_t slot, int32_t energy_slot, 
   AMA_CUDA_TRY(cudaFuncSetAttribute(grid_g2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
   auto T = [&](int axis, int dir) { return (const double2*)e->d.tw[AMA_C128][axis][dir]; };
   const double invN = 1.0 / (double)e->N;
-  grid_g1_kernel<<<g.n1, kFftThreads, ps, s>>>(g, T(1, 1), T(2, 1), in, g_grid_work);
+  grid_g1_kernel<<<g.n1, kFftThreads, ps, s>>>(g, T(1, 1), T(2, 1), in, e->grid_work);
   AMA_CHECK_LAUNCH();
-  grid_g2_kernel<<<g.n2, kFftThreads, ss, s>>>(g, T(0, 1), T(0, 0), it->second.filt[slot], ef, invN,
-                                                  invN * invN, g_grid_work, energy);
+  grid_g2_kernel<<<g.n2, kFftThreads, ss, s>>>(g, T(0, 1), T(0, 0), e->grid_filt[slot], ef, invN,
+                                                  invN * invN, e->grid_work, energy);
   AMA_CHECK_LAUNCH();
-  grid_g3_kernel<<<g.n1, kFftThreads, ps, s>>>(g, T(1, 0), T(2, 0), g_grid_work, out);
+  grid_g3_kernel<<<g.n1, kFftThreads, ps, s>>>(g, T(1, 0), T(2, 0), e->grid_work, out);
   AMA_CHECK_LAUNCH();
   return AMA_OK;
 }
@@ -1315,22 +1337,17 @@ extern "C" int ama_grid_filter(AmaEngine* e, int32_t slot, int32_t energy_slot, 
 extern "C" int ama_grid_fft_forward(AmaEngine* e, const double* in, void* out, void* stream) {
   AMA_REQUIRE(e && in && out, AMA_ERR_ARG, "null argument");
   AMA_REQUIRE(e->precisions & (1u << AMA_C128), AMA_ERR_ARG, "grid transforms need the complex128 tables");
+  if (int rc = require_engine_device(e)) return rc;
   cudaStream_t s = (cudaStream_t)stream;
-  const size_t need = (size_t)e->N * sizeof(double2);
-  if (g_grid_work_bytes < need) {
-    if (g_grid_work) cudaFree(g_grid_work);
-    g_grid_work = nullptr; g_grid_work_bytes = 0;
-    AMA_CUDA_TRY(cudaMalloc((void**)&g_grid_work, need));
-    g_grid_work_bytes = need;
-  }
+  if (int rc = ensure_grid_work(e)) return rc;
   GridView g = grid_view(e);
   const size_t ps = plane_smem<double>(e), ss = slab_smem<double>(e);
   AMA_CUDA_TRY(cudaFuncSetAttribute(grid_g1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
   AMA_CUDA_TRY(cudaFuncSetAttribute(grid_g2f_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
   auto T = [&](int axis, int dir) { return (const double2*)e->d.tw[AMA_C128][axis][dir]; };
-  grid_g1_kernel<<<g.n1, kFftThreads, ps, s>>>(g, T(1, 1), T(2, 1), in, g_grid_work);
+  grid_g1_kernel<<<g.n1, kFftThreads, ps, s>>>(g, T(1, 1), T(2, 1), in, e->grid_work);
   AMA_CHECK_LAUNCH();
-  grid_g2f_kernel<<<g.n2, kFftThreads, ss, s>>>(g, T(0, 1), g_grid_work, (double2*)out, 1.0 / (double)e->N);
+  grid_g2f_kernel<<<g.n2, kFftThreads, ss, s>>>(g, T(0, 1), e->grid_work, (double2*)out, 1.0 / (double)e->N);
   AMA_CHECK_LAUNCH();
   return AMA_OK;
 }
@@ -1367,17 +1384,40 @@ extern "C" int ama_engine_option(AmaEngine* e, int32_t option, int32_t value) {
 // ama_grid_filter with its complex work grid in a fixed file-scope device array instead
 // of the lazily grown allocation. The array holds kNoAllocGridPoints complex FP64 values
 // (128^3 points, 32 MiB) and lives on every GPU that loads the library until the process
-// exits. The first call on a device looks up the array's device address
-// (cudaGetSymbolAddress, with that device current); make that first call before any
-// stream capture. Every call shares the array and overwrites it completely before reading
-// it, so nothing needs clearing between calls; calls that overlap on the GPU (different
-// streams, no ordering between them) race on the array.
+// exits. Its device address is looked up (cudaGetSymbolAddress, with the device current)
+// when an engine is created on that device, which also loads the library's device code
+// there under lazy module loading, so the array is in place before a framework allocator
+// reserves the rest of the GPU; a call on a device without an engine looks it up on its
+// first use, which should then come before any stream capture. The library does not
+// survive a cudaDeviceReset of a device it has used. Every call shares the array and
+// overwrites it completely before reading it, so nothing needs clearing between calls;
+// calls that overlap on the GPU (different streams, no ordering between them) race on the
+// array.
 namespace {
 constexpr int64_t kNoAllocGridPoints = 128 * 128 * 128;
 __device__ __align__(256) double2 g_noalloc_grid[kNoAllocGridPoints];
-constexpr int kMaxDevices = 64;
-void* g_noalloc_addr[kMaxDevices] = {};
+std::atomic<void*> g_noalloc_addr[kMaxDevices];
+
+// The array's device address on the current device (looked up once per device).
+int noalloc_address(double2** out) {
+  const int dev = current_device();
+  AMA_REQUIRE(dev >= 0, AMA_ERR_UNSUPPORTED, "device index out of range");
+  void* addr = g_noalloc_addr[dev].load(std::memory_order_acquire);
+  if (!addr) {
+    AMA_CUDA_TRY(cudaGetSymbolAddress(&addr, g_noalloc_grid));
+    g_noalloc_addr[dev].store(addr, std::memory_order_release);  // every thread finds the same address
+  }
+  *out = static_cast<double2*>(addr);
+  return AMA_OK;
+}
 }  // namespace
+
+namespace ama {
+int noalloc_prepare() {
+  double2* unused = nullptr;
+  return noalloc_address(&unused);
+}
+}  // namespace ama
 
 extern "C" int ama_grid_filter_noalloc(AmaEngine* e, int32_t slot, int32_t energy_slot, const double* in,
                                        double* out, double* energy, void* stream) {
@@ -1386,22 +1426,15 @@ extern "C" int ama_grid_filter_noalloc(AmaEngine* e, int32_t slot, int32_t energ
   AMA_REQUIRE(e->N <= kNoAllocGridPoints, AMA_ERR_SHAPE,
               "ama_grid_filter_noalloc: grid of " + std::to_string(e->N) + " points exceeds the fixed work array of " +
                   std::to_string(kNoAllocGridPoints) + " points (use ama_grid_filter)");
-  auto it = g_filters.find(e);
-  AMA_REQUIRE(it != g_filters.end() && it->second.filt[slot], AMA_ERR_ARG, "filter slot not set");
+  AMA_REQUIRE(e->grid_filt[slot], AMA_ERR_ARG, "filter slot not set");
   const double* ef = nullptr;
   if (energy_slot >= 0) {
-    ef = it->second.filt[energy_slot];
+    ef = e->grid_filt[energy_slot];
     AMA_REQUIRE(ef && energy, AMA_ERR_ARG, "energy filter slot not set or energy is null");
   }
-  int dev = 0;
-  AMA_CUDA_TRY(cudaGetDevice(&dev));
-  AMA_REQUIRE(dev >= 0 && dev < kMaxDevices, AMA_ERR_UNSUPPORTED, "device index out of range");
-  if (!g_noalloc_addr[dev]) {
-    void* addr = nullptr;
-    AMA_CUDA_TRY(cudaGetSymbolAddress(&addr, g_noalloc_grid));
-    g_noalloc_addr[dev] = addr;
-  }
-  double2* work = static_cast<double2*>(g_noalloc_addr[dev]);
+  if (int rc = require_engine_device(e)) return rc;
+  double2* work = nullptr;
+  if (int rc = noalloc_address(&work)) return rc;
   cudaStream_t s = (cudaStream_t)stream;
   GridView g = grid_view(e);
   const size_t ps = plane_smem<double>(e), ss = slab_smem<double>(e);
@@ -1412,7 +1445,7 @@ extern "C" int ama_grid_filter_noalloc(AmaEngine* e, int32_t slot, int32_t energ
   const double invN = 1.0 / (double)e->N;
   grid_g1_kernel<<<g.n1, kFftThreads, ps, s>>>(g, T(1, 1), T(2, 1), in, work);
   AMA_CHECK_LAUNCH();
-  grid_g2_kernel<<<g.n2, kFftThreads, ss, s>>>(g, T(0, 1), T(0, 0), it->second.filt[slot], ef, invN, invN * invN,
+  grid_g2_kernel<<<g.n2, kFftThreads, ss, s>>>(g, T(0, 1), T(0, 0), e->grid_filt[slot], ef, invN, invN * invN,
                                                 work, energy);
   AMA_CHECK_LAUNCH();
   grid_g3_kernel<<<g.n1, kFftThreads, ps, s>>>(g, T(1, 0), T(2, 0), work, out);

@@ -79,6 +79,14 @@ struct AmaEngine {
   const void* b_variant[2][3] = {};  // [prec] stage B variants compiled for the grid
   NlTcState tc;
   bool use_tc = true;
+  // FP64 grid transforms (Hartree, Kerker): reciprocal-space filters in the engine's
+  // permuted order, and the complex work grid of ama_grid_filter / ama_grid_fft_forward.
+  // Both live on the engine's device; calls on one engine from different streams race on
+  // the work grid.
+  double* grid_filt[4] = {};
+  double2* grid_work = nullptr;
+  size_t grid_work_bytes = 0;
+  int device = 0;
 };
 
 namespace ama {
@@ -90,6 +98,8 @@ int nl_tc_run(AmaEngine* e, int k_first, int k_count, int nbands, const float2* 
 int nl_tc_apply(AmaEngine* e, int k_first, int k_count, int nbands, float2* hpsi, cudaStream_t s, int ntile,
                 int bn);
 void nl_tc_free(AmaEngine* e);
+// look up the allocation-free grid array on the current device (once per device)
+int noalloc_prepare();
 }  // namespace ama
 
 

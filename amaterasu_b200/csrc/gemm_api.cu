@@ -21,7 +21,7 @@ template <typename C> struct StridedBatch {
 };
 
 struct Scratch { void* ptr = nullptr; size_t bytes = 0; };
-thread_local Scratch g_partial;
+thread_local PerDevice<Scratch> g_partial_dev;  // per host thread and device
 
 template <typename T>
 int zgemm_impl(int form, int m, int n, int k, const double* alpha, const void* a, int64_t lda,
@@ -34,6 +34,9 @@ int zgemm_impl(int form, int m, int n, int k, const double* alpha, const void* a
   int splits = std::max(1, std::min(32, (2 * 148 + tiles - 1) / tiles));
   splits = std::min(splits, std::max(1, k / 512));
   const int64_t pstride = (int64_t)m * n;
+  Scratch* gpd = g_partial_dev.here();
+  AMA_REQUIRE(gpd, AMA_ERR_CUDA, "complex GEMM: no usable current CUDA device");
+  Scratch& g_partial = *gpd;
   if (splits > 1) {
     const size_t need = (size_t)batch * splits * pstride * sizeof(double2);
     if (g_partial.bytes < need) {
@@ -132,6 +135,9 @@ int kbatch_impl(int form, int nk, int m, int n, int k, const int32_t* npw, const
     splits = std::max(1, std::min(32, (2 * 148 + tiles - 1) / tiles));
   }
   const int64_t pstride = (int64_t)max_m * max_n;
+  Scratch* gpd = g_partial_dev.here();
+  AMA_REQUIRE(gpd, AMA_ERR_CUDA, "complex GEMM: no usable current CUDA device");
+  Scratch& g_partial = *gpd;
   if (splits > 1) {
     const size_t need = (size_t)nk * splits * pstride * sizeof(double2);
     if (g_partial.bytes < need) {

@@ -27,6 +27,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <atomic>
 #include <string>
 
 using namespace ama;
@@ -218,22 +219,26 @@ struct TcScratch {
   Buf a, b, part;
   int* err = nullptr;
 };
-thread_local TcScratch g_tc;
+thread_local PerDevice<TcScratch> g_tc_dev;  // per host thread and device
+PerDevice<std::atomic<int>> g_tc_attrs;       // kernel attributes set on this device
 
 int tile_n(int cols) { return cols >= kChainBN ? kChainBN : std::max(16, round_up(cols, 16)); }
 
 int ensure_err() {
+  TcScratch* gt = g_tc_dev.here();
+  AMA_REQUIRE(gt, AMA_ERR_CUDA, "tensor-core subspace GEMM: no usable current CUDA device");
+  TcScratch& g_tc = *gt;
   if (!g_tc.err) {
     AMA_CUDA_TRY(cudaMalloc((void**)&g_tc.err, sizeof(int)));
     AMA_CUDA_TRY(cudaMemset(g_tc.err, 0, sizeof(int)));
   }
-  static bool attrs = false;
-  if (!attrs) {
+  std::atomic<int>& attrs = *g_tc_attrs.here();
+  if (!attrs.load()) {
     AMA_CUDA_TRY(cudaFuncSetAttribute(tc_chain_kernel<kChainPartial>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       kChainSmemCap));
     AMA_CUDA_TRY(cudaFuncSetAttribute(tc_chain_kernel<kChainComplexNN>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, kChainSmemCap));
-    attrs = true;
+    attrs.store(1);
   }
   return AMA_OK;
 }
@@ -241,6 +246,8 @@ int ensure_err() {
 int run_nc(int nk, int m, int n, const int32_t* npw, const int64_t* pw_off, const AmaKOperand* a,
            const AmaKOperand* b, const AmaKOperand* c, const double* alpha, const double* beta, int max_npw,
            cudaStream_t s) {
+  if (int rc = ensure_err()) return rc;
+  TcScratch& g_tc = *g_tc_dev.here();
   const int mpad = round_up(m, 64);
   const int rows_a = 2 * mpad;
   const int bn = tile_n(n);
@@ -292,6 +299,8 @@ int run_nc(int nk, int m, int n, const int32_t* npw, const int64_t* pw_off, cons
 int run_nn(int nk, int m, int kdim, const int32_t* npw, const int64_t* pw_off, const AmaKOperand* a,
            const AmaKOperand* b, const AmaKOperand* c, const double* alpha, const double* beta, int max_npw,
            cudaStream_t s) {
+  if (int rc = ensure_err()) return rc;
+  TcScratch& g_tc = *g_tc_dev.here();
   const int gpad = round_up(max_npw, kBM);
   const int kp = round_up(2 * kdim, kBK);
   const int bn = tile_n(2 * m);
@@ -362,6 +371,7 @@ extern "C" int ama_kbatch_zgemm_tc(int32_t form, int32_t nk, int32_t m, int32_t 
 extern "C" int ama_subspace_tc_status(int32_t* code) {
   AMA_REQUIRE(code, AMA_ERR_ARG, "null argument");
   *code = 0;
-  if (g_tc.err) AMA_CUDA_TRY(cudaMemcpy(code, g_tc.err, sizeof(int), cudaMemcpyDeviceToHost));
+  TcScratch* gt = g_tc_dev.here();
+  if (gt && gt->err) AMA_CUDA_TRY(cudaMemcpy(code, gt->err, sizeof(int), cudaMemcpyDeviceToHost));
   return AMA_OK;
 }

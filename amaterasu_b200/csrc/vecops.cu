@@ -147,7 +147,7 @@ __global__ void lda_pz_kernel(const double* __restrict__ rho, int64_t npts, doub
 }
 
 struct MapScratch { int* ptr = nullptr; int n = 0; };
-thread_local MapScratch g_map;
+thread_local PerDevice<MapScratch> g_map_dev;  // per host thread and device
 
 }  // namespace
 
@@ -162,6 +162,9 @@ extern "C" int ama_residual_precondition(int32_t precision, int32_t nbands, int3
   cudaStream_t s = (cudaStream_t)stream;
   int* map = nullptr;
   if (nrows > 0) {
+    MapScratch* gm = g_map_dev.here();
+    AMA_REQUIRE(gm, AMA_ERR_CUDA, "no usable current CUDA device");
+    MapScratch& g_map = *gm;
     if (g_map.n < nbands) {
       if (g_map.ptr) cudaFree(g_map.ptr);
       g_map.ptr = nullptr; g_map.n = 0;

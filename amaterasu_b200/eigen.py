@@ -10,7 +10,7 @@ once the subspace would exceed subspace_factor*nbands}.
 
 All block products run on the engine's GEMM kernels in the working precision (complex128
 by default, complex64 for the mixed-precision policy); the small projected problems are
-solved in FP64 (cuSOLVER). The reference's thin SVD in ``orthogonalize_against`` is
+solved in FP64 (hand-written eigensolver and Cholesky kernels). The reference's thin SVD in ``orthogonalize_against`` is
 replaced by the equivalent eigendecomposition of the Gram matrix (same kept span and
 threshold semantics: singular values above threshold * largest) followed by one
 Cholesky re-orthonormalisation.

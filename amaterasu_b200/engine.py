@@ -165,6 +165,36 @@ class DeviceEngine:
         return out
 
 
+class DeviceTimeout(_lib.AmaError):
+    """A bounded device-side wait ran out: the kernel skipped the rest of its work, so the
+    results of that launch (and everything computed from them) are wrong."""
+
+
+def check_device_status(engine: "DeviceEngine | None" = None) -> None:
+    """Raise :class:`DeviceTimeout` if a kernel recorded a timed-out wait.
+
+    The tcgen05 kernels (nonlocal products of an engine, Davidson subspace products of the
+    current device) bound every mbarrier wait, and the eigensolver's cooperative
+    tridiagonalisation bounds every grid-barrier wait; one that runs out sets a device-side
+    error word and the kernel returns without finishing. Reading the words costs one small
+    synchronous device-to-host copy each, so callers check once per SCF step."""
+    codes = []
+    code = ct.c_int32(0)
+    if engine is not None:
+        call("ama_tc_status", engine.handle, ct.byref(code))
+        codes.append(("nonlocal tensor-core products", int(code.value)))
+    code = ct.c_int32(0)
+    call("ama_subspace_tc_status", ct.byref(code))
+    codes.append(("subspace tensor-core products", int(code.value)))
+    code = ct.c_int32(0)
+    call("ama_solver_status", ct.byref(code))
+    codes.append(("subspace eigensolver", int(code.value)))
+    bad = [f"{name} (wait code {value})" for name, value in codes if value]
+    if bad:
+        raise DeviceTimeout("a bounded device wait ran out in the " + " and ".join(bad)
+                            + "; the results of that step are invalid")
+
+
 def engine_for(system, precisions=("complex128", "complex64")) -> DeviceEngine:
     """The system's engine, created on first use and cached on the system object."""
     eng = getattr(system, "_device_engine", None)

@@ -1,9 +1,9 @@
 """Device linear algebra for the subspace steps, on the engine's own kernels.
 
 GEMMs go to ``ama_zgemm`` (hand-written complex GEMM, FP32 or FP64 by dtype); the small
-dense FP64 factorisations (Hermitian eigensolve, inverse Cholesky factor) go to
-``ama_heev`` / ``ama_potrf_inv`` (cuSOLVER, the LAPACK routines the reference reaches
-through scipy). All tensors are CUDA torch tensors, row-major, contiguous.
+dense FP64 factorisations (Hermitian eigensolve, inverse Cholesky factor) go to the
+hand-written ``ama_heev`` / ``ama_potrf_inv`` (they stand in for the LAPACK routines the
+reference reaches through scipy). All tensors are CUDA torch tensors, row-major, contiguous.
 """
 from __future__ import annotations
 

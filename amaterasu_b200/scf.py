@@ -31,14 +31,14 @@ from .batched import BatchedDavidson
 from .config import Config, parse_energy
 from .density import accumulate_packed, band_weights, finalize_density
 from .eigen import davidson, random_bands
-from .engine import engine_for, require_cuda
+from .engine import check_device_status, engine_for, require_cuda
 from .hamiltonian import Hamiltonian
 from .mixing import create_mixer
 from .occupations import compute_occupations
 from .potential import effective_potential, grid_ops
 from .units import EV_IN_HARTREE, HARTREE_IN_EV
 
-__all__ = ["Energies", "SCFResult", "run_scf"]
+__all__ = ["Energies", "SCFResult", "prepare_starting_orbitals", "run_scf", "starting_orbitals"]
 
 
 @dataclass
@@ -105,6 +105,32 @@ class _Orbitals:
     def to(self, dtype):
         self.packed = [p.to(dtype) for p in self.packed]
         self.dtype = dtype
+
+
+def starting_orbitals(system, spin: int, ik: int) -> torch.Tensor:
+    """The reference's seeded starting block of (spin, k): random_bands seeded
+    12345 + 991 spin + ik (scf/driver.py:255-264), orthonormalised, complex128 on the device.
+
+    It depends only on the system (plane-wave count, kinetic energies, band count), so it is
+    drawn once per system and kept: every SCF run on the system, whatever its precision
+    policy, starts from the same block without drawing it again. ``prepare_starting_orbitals``
+    draws them all up front (part of the system set-up)."""
+    cache = system.__dict__.setdefault("_start_orbitals", {})
+    key = (spin, ik, system.nbands)
+    block = cache.get(key)
+    if block is None:
+        sphere = system.wave_spheres[ik]
+        block = random_bands(len(sphere), system.nbands, sphere.kinetic_energy, seed=12345 + 991 * spin + ik,
+                             dtype=torch.complex128)
+        cache[key] = block
+    return block
+
+
+def prepare_starting_orbitals(system) -> None:
+    """Draw every (spin, k) starting block of the system now (see starting_orbitals)."""
+    for spin in range(system.nspin):
+        for ik in range(system.nkpoints):
+            starting_orbitals(system, spin, ik)
 
 
 def _kinetic_energy(system, orb: _Orbitals, occ, kin_dev) -> float:
@@ -184,8 +210,7 @@ def run_scf(system, config: Config | None = None, *, logger=None, wavefunctions=
                 w = w if isinstance(w, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(w))
                 orb.set(spin, ik, w.to(dev, wdtype))
             else:
-                orb.set(spin, ik, random_bands(len(sphere), nb, sphere.kinetic_energy,
-                                               seed=12345 + 991 * spin + ik, dtype=wdtype))
+                orb.set(spin, ik, starting_orbitals(system, spin, ik).to(wdtype))
     eng.reserve("complex128" if wdtype == torch.complex128 else "complex64", nb)
     kin_dev = [torch.from_numpy(s.kinetic_energy).to(dev) for s in system.wave_spheres]
     dij_dev = torch.from_numpy(system.projectors[0].dij).to(dev, torch.complex128) if eng.nproj else None
@@ -244,6 +269,7 @@ def run_scf(system, config: Config | None = None, *, logger=None, wavefunctions=
                                kin_dev[ik], tolerance=tol, max_iterations=maxit)
                 eigenvalues[spin, ik] = res.eigenvalues.cpu().numpy()
                 orb.set(spin, ik, res.coefficients)
+        check_device_status(eng)  # a timed-out device wait must not go unnoticed
         if distributed:
             eig_all = comm.gather_eigenvalues(eigenvalues, system.kparts)
             weights_all = system.global_weights

@@ -13,7 +13,8 @@ residual below 1e-7 per electron:
 * ``learned+mixed`` (with ``--weights``): the mixed policy from the learned start density,
   the network run on a working grid with the spacing it was trained at (0.151 A).
 
-Reported per run: SCF seconds (system set-up excluded, the same for every run),
+Reported per run: SCF seconds (system set-up excluded, the same for every run: grids,
+spheres, projectors, structure factors and the seeded starting orbitals),
 iterations, free energy, |dF| per atom against the plain run, and the largest force
 (eV/A) and stress (GPa) differences against the plain run when ``--forces`` / ``--stress``
 are given.
@@ -67,9 +68,11 @@ def run(workload: str, weights=None, forces=False, log=print, policies=("plain",
         engine_options=None, spacing=TRAINING_SPACING_A, stress=False) -> dict:
     import torch
     from .learned import DensityNet, LearnedStart, working_grid
-    from .scf import run_scf
+    from .scf import prepare_starting_orbitals, run_scf
     t0 = time.perf_counter()
     system = _system(workload)
+    prepare_starting_orbitals(system)  # the seeded start is part of the system, same for every policy
+    torch.cuda.synchronize()
     setup = time.perf_counter() - t0
     runs = [(p, {"plain": "complex128"}.get(p, "mixed"), None) for p in policies if p in ("plain", "mixed")]
     if weights and "learned+mixed" in policies:

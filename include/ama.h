@@ -225,18 +225,28 @@ AMA_API int ama_lda_pz(const double* rho, int64_t npoints, double* eps, double* 
 AMA_API int ama_structure_sum(const double* gcart, int32_t ng, const double* positions, const int32_t* species,
                               int32_t natoms, const double* radial, double scale, double* out, void* stream);
 
-/* Dense FP64 Hermitian eigensolver for `batch` matrices of order n (device, row-major,
- * interleaved complex, overwritten by eigenvectors as columns); eigenvalues ascending.
- * Replaces scipy.linalg.eigh in rayleigh_ritz (scf/eigen/subspace.py:74). */
+/* Dense FP64 Hermitian eigensolver for `batch` matrices of order n <= 3456 (device,
+ * row-major, interleaved complex, overwritten by eigenvectors as columns); eigenvalues
+ * ascending. Hand-written: Householder tridiagonalisation in one cooperative launch,
+ * multisection bisection, inverse iteration with Gram-Schmidt inside eigenvalue clusters,
+ * back-transformation; no vendor solver library and no host synchronisation (a device-side
+ * failure is reported by ama_solver_status). Scratch grows on demand per host thread and
+ * device. Replaces scipy.linalg.eigh in rayleigh_ritz (scf/eigen/subspace.py:74). */
 AMA_API int ama_heev(int32_t n, void* matrices, double* eigenvalues, int32_t batch, void* stream);
 
 /* The lowest nvec eigenpairs of each matrix (as ama_heev: eigenvalues ascending in
  * eigenvalues[b*n + 0 .. nvec), eigenvectors in row-major columns 0 .. nvec-1; the rest of
- * both is undefined). Bisection and inverse iteration on the tridiagonal form (zheevdx):
- * the Rayleigh-Ritz step needs only the nbands lowest of m = up to 5 nbands Ritz pairs
+ * both is undefined). Only nvec eigenvalues are bisected and nvec vectors back-transformed:
+ * the Rayleigh-Ritz step needs the nbands lowest of m = up to 5 nbands Ritz pairs
  * (subspace.py:74 computes all of them with scipy.linalg.eigh). */
 AMA_API int ama_heev_lowest(int32_t n, int32_t nvec, void* matrices, double* eigenvalues, int32_t batch,
                             void* stream);
+
+/* Sticky device-side status of ama_heev/ama_heev_lowest on the current device and host
+ * thread (0 = fine, 1 = a bounded grid-barrier wait ran out, so the results of some call
+ * since the last read are invalid); synchronous; clears the word. No counterpart in the
+ * reference. */
+AMA_API int ama_solver_status(int32_t* code);
 
 /* The same for many small matrices (order n <= 80) at once: one CTA per matrix, cyclic
  * Jacobi in shared memory, FP64. Used for the per-k-point Rayleigh-Ritz problems of the
@@ -245,8 +255,9 @@ AMA_API int ama_heev_small(int32_t n, void* matrices, double* eigenvalues, int32
 
 /* Inverse Cholesky factor of `batch` Hermitian positive-definite FP64 matrices (device,
  * row-major, interleaved complex): on return each holds L^{-1} (lower triangular) with
- * S = L L^H. AMA_ERR_NOT_SPD if a pivot is not positive. Replaces the cholesky +
- * solve_triangular pair of orthonormalize (scf/eigen/subspace.py:17-32). */
+ * S = L L^H. AMA_ERR_NOT_SPD if a pivot is not positive (synchronous: the caller falls back
+ * on it). Hand-written, one CTA per matrix. Replaces the cholesky + solve_triangular pair of
+ * orthonormalize (scf/eigen/subspace.py:17-32). */
 AMA_API int ama_potrf_inv(int32_t n, void* matrices, int32_t batch, void* stream);
 
 /* ---- learned start density: periodic 3D convolution network (no counterpart in the

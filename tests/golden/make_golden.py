@@ -15,6 +15,12 @@ Fixtures (``*.npz``):
   si64.npz      Si64 40 Ry, Gamma + 3 random k: sphere and projector pins, v_eff
                 checksums, H.psi of a few bands
   si8_k.npz     Si8 displaced, 8x8x8 Gamma mesh: k-points, weights, plane-wave counts
+  si8_scf1.npz  the same Si8 cell at 40 Ry, 260 k-points, 20 bands, Fermi-Dirac 0.01 Ha:
+                the first SCF iteration from the reference's own start (eigenvalues at
+                every k, energy terms, output-density checksums and probes)
+  si215.npz     Si215 (3x3x3 conventional, one vacancy, displaced), Gamma, 30 Ry, 440
+                bands: sphere and projector pins, Ewald energy/forces/stress, v_eff
+                checksums and probes, starting-orbital pins, H.psi of a few bands
 """
 from __future__ import annotations
 
@@ -252,13 +258,88 @@ def make_si8(pseudo, out):
                         positions=s.positions)
 
 
+# ---------------------------------------------------------------------- si8_scf1
+def make_si8_scf1(pseudo, out):
+    from amaterasu.scf.driver import run_scf
+    from amaterasu_b200.cells import workload
+
+    structure, ecut, _, nbands = workload("si8_batched")
+    cfg = _config(kpoints__grid=[8, 8, 8], occupations__scheme="fermi-dirac",
+                  occupations__smearing="0.01 Ha", occupations__nbands=nbands,
+                  scf__max_steps=1)
+    t0 = time.perf_counter()
+    system = _system(structure, cfg, pseudo, ecut)
+    setup = time.perf_counter() - t0
+    result = run_scf(system, cfg, logger=print)
+    e = result.energies
+    rng = np.random.default_rng(81)
+    probe = rng.integers(0, result.density.size, size=400)
+    np.savez_compressed(
+        out / "si8_scf1.npz", grid=np.array(system.grid.shape), kpoints=system.kpoints.points,
+        weights=system.kpoints.weights, npw=np.array([len(s) for s in system.wave_spheres]),
+        ewald=system.ewald, e_kinetic=e.kinetic, e_local=e.local, e_hartree=e.hartree,
+        e_xc=e.xc, e_nonlocal=e.nonlocal_, e_entropy=e.entropy, e_free=e.free_energy,
+        eigenvalues=result.eigenvalues, occupations=result.occupations, fermi=result.fermi_level,
+        history=np.array(result.history), probe=probe, density_probe=result.density.ravel()[probe],
+        density_sum=float(result.density.sum()), density_sq=float((result.density**2).sum()),
+        seconds_setup=setup, seconds_scf=result.seconds)
+
+
+# ------------------------------------------------------------------------- si215
+def make_si215(pseudo, out):
+    from amaterasu.hamiltonian.ewald import ewald
+    from amaterasu.hamiltonian.operator import Hamiltonian
+    from amaterasu.scf.driver import effective_potential
+    from amaterasu.scf.eigen import random_bands
+    from amaterasu_b200.cells import workload
+
+    structure, ecut, _, nbands = workload("si215_gamma")
+    cfg = _config(kpoints__scheme="gamma", occupations__scheme="gaussian",
+                  occupations__smearing="0.005 Ha", occupations__nbands=nbands)
+    t0 = time.perf_counter()
+    system = _system(structure, cfg, pseudo, ecut)
+    setup = time.perf_counter() - t0
+    print(f"si215 set-up {setup:.1f} s", flush=True)
+    charges = np.full(len(system.symbols), 4.0)
+    ew = ewald(system.cell, system.positions, charges)
+    rho0 = system.initial_density()
+    veff, e_h, e_xc, _ = effective_potential(system, rho0)
+    rng = np.random.default_rng(215)
+    probe = rng.integers(0, veff.size, size=400)
+    sphere = system.wave_spheres[0]
+    B = system.projectors[0].matrix
+    d = dict(grid=np.array(system.grid.shape), npw=np.array([len(sphere)]),
+             miller_sha=np.array([_sha(sphere.miller.astype(np.int64))]), nproj=len(B),
+             ewald=system.ewald, ewald_energy=ew.energy, ewald_forces=ew.forces, ewald_stress=ew.stress,
+             positions=system.positions, cell=system.cell, seconds_setup=setup,
+             e_hartree0=e_h, e_xc0=e_xc, probe=probe, veff_probe=veff.ravel()[probe],
+             veff_sum=float(veff.sum()), veff_sq=float((veff**2).sum()),
+             vloc_probe=system.v_local.ravel()[probe], rho0_probe=rho0.ravel()[probe],
+             rho0_sum=float(rho0.sum()), proj_norms=np.linalg.norm(B, axis=1),
+             proj_row0=B[0, :64], proj_row859=B[-1, :64])
+    t0 = time.perf_counter()
+    start = random_bands(len(sphere), nbands, sphere.kinetic_energy, seed=12345)
+    d["seconds_random_bands"] = time.perf_counter() - t0
+    d["start_row0"] = start[0, :256]
+    d["start_row_last"] = start[-1, :256]
+    d["start_col_norms"] = np.linalg.norm(start[:, :512], axis=0)
+    del start
+    H = Hamiltonian(system, veff)
+    psi = damped_noise(len(sphere), 3, sphere.kinetic_energy, 2150)
+    t0 = time.perf_counter()
+    d["hpsi"] = H.apply(psi, 0)
+    d["seconds_hpsi3"] = time.perf_counter() - t0
+    np.savez_compressed(out / "si215.npz", **d)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
     ap.add_argument("--only", nargs="*", default=None)
     args = ap.parse_args()
     _import_reference(args.reference)
-    jobs = {"mini": make_mini, "si8": make_si8, "si64": make_si64, "si2": make_si2}
+    jobs = {"mini": make_mini, "si8": make_si8, "si64": make_si64, "si2": make_si2,
+            "si215": make_si215, "si8_scf1": make_si8_scf1}
     with tempfile.TemporaryDirectory() as tmp:
         pseudo, _ = _upf(tmp)
         for name, job in jobs.items():
