@@ -77,6 +77,13 @@ SIGNATURES = {
     "ama_heev": (ct.c_int, [_I32, _P, _P, _I32, _P]),
     "ama_heev_lowest": (ct.c_int, [_I32, _I32, _P, _P, _I32, _P]),
     "ama_solver_status": (ct.c_int, [ct.POINTER(ct.c_int32)]),
+    "ama_vec_gram": (ct.c_int, [_I32, _P, _I32, _P, _P, _I64, _P, _P]),
+    "ama_vec_lincomb": (ct.c_int, [_I32, _P, _P, _I64, _P, _P]),
+    "ama_vec_reduce": (ct.c_int, [_I32, _I64, _P, _P, _D, _I32, _P, _P]),
+    "ama_density_floor": (ct.c_int, [_I32, _I64, _D, _P, _P]),
+    "ama_band_kinetic": (ct.c_int, [_I32, _I32, _I32, _P, _P, _P, _P, _P, _P]),
+    "ama_rowdot": (ct.c_int, [_I32, _I32, _P, _P, _P, _P]),
+    "ama_ewald": (ct.c_int, [_I32, _P, _P, _P, _I32, _P, _I32, _D, _D, _D, _P, _P, _P]),
     "ama_structure_sum": (ct.c_int, [_P, _I32, _P, _P, _I32, _P, ct.c_double, _P, _P]),
     "ama_potrf_inv": (ct.c_int, [_I32, _P, _I32, _P]),
     "ama_heev_small": (ct.c_int, [_I32, _P, _P, _I32, _P]),

@@ -64,6 +64,7 @@ class BatchedDavidson:
         # complex64 plane-wave products on the tensor cores (split-TF32) once the spheres are
         # long enough for the staged tiles to pay; shorter ones stay on the SIMT kernels
         self.tensor_cores = bool(tensor_cores) and dtype == torch.complex64 and self.max_npw >= tc_min_npw
+        self.trace = []  # per iteration of the last run: (iteration, active directions, subspace size, max norm)
 
     # ---------------------------------------------------------------- kernels
     def _gemm(self, form, m, n, k, a: _KOp, b: _KOp, c: _KOp, alpha=1.0, beta=0.0, max_m=None, max_n=None):
@@ -202,6 +203,7 @@ class BatchedDavidson:
         """Lowest nbands eigenpairs at every k. ``guess_packed`` packs one (nbands, npw_k)
         block per k; returns (eigenvalues [nk][nb] numpy, X packed, norms numpy, iterations)."""
         nb, cap = self.nb, self.cap
+        self.trace = []
         H._bind()
         guess = guess_packed.to(self.dtype).contiguous()
         # the guess is usually the previous step's orthonormal orbitals: polish them without a
@@ -229,6 +231,7 @@ class BatchedDavidson:
             active = norms > tolerance
             counts = active.sum(axis=1)
             nn = int(counts.max())
+            self.trace.append((it, nn, m, float(norms.max())))
             if nn == 0:
                 break
             rows = np.full((self.nk, nb), -1, dtype=np.int32)
@@ -246,6 +249,7 @@ class BatchedDavidson:
                            alpha=-1.0, beta=1.0)
             new, keep1 = self._orthonormal_rows(C, nn, 1e-7, True)
             if not keep1.any():
+                self.trace.append((it, 0, m, -1.0))  # every new direction was dependent
                 break
             polished = self._lowdin_rows(new, nn, keep1)
             if polished is not None:

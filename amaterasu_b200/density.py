@@ -37,16 +37,17 @@ def accumulate_packed(system, packed: torch.Tensor, nbands: int, weights: np.nda
 
 
 def finalize_density(system, rho: torch.Tensor, symmetrize: bool = True) -> torch.Tensor:
-    """Divide by Omega; floor at zero and rescale each channel to its charge."""
-    rho = rho / system.grid.volume
+    """Divide by Omega; with ``symmetrize`` (symmetry being off, only the floor) also floor at
+    zero and rescale each channel to its charge (``ama_density_floor``, in place)."""
+    from ._lib import call
+    from .engine import ptr, stream_ptr
+    rho = rho.contiguous()
+    nch, n = rho.shape[0], rho[0].numel()
     if symmetrize:
-        before = rho.sum(dim=1)
-        clipped = torch.clamp(rho, min=0.0)
-        after = clipped.sum(dim=1)
-        scale = torch.where(after > 0, before / torch.where(after > 0, after, torch.ones_like(after)),
-                            torch.ones_like(after))
-        rho = clipped * scale[:, None]
-    return rho
+        call("ama_density_floor", nch, n, float(system.grid.volume), ptr(rho), stream_ptr())
+        return rho
+    from .mixing import _lincomb
+    return _lincomb([rho.reshape(-1)], [1.0 / system.grid.volume]).reshape(rho.shape)
 
 
 def compute_density(system, wavefunctions, occupations, *, symmetrize: bool = True):

@@ -195,6 +195,41 @@ def check_device_status(engine: "DeviceEngine | None" = None) -> None:
                             + "; the results of that step are invalid")
 
 
+class GridEngine:
+    """A C-ABI engine for a bare FFT grid (one plane wave, no projectors): enough for the
+    FP64 grid transforms and filters (Kerker, Hartree) when no system engine exists."""
+
+    def __init__(self, shape):
+        self.device = require_cuda()
+        lib = _lib.load()
+        self.grid_shape = tuple(int(n) for n in shape)
+        self.N = int(np.prod(self.grid_shape))
+        npw = np.ones(1, dtype=np.int32)
+        miller = np.zeros(3, dtype=np.int32)
+        kinetic = np.zeros(1)
+        dij = np.zeros(1)
+        self._keep = (npw, miller, kinetic, dij)
+        desc = _lib.AmaSystemDesc(
+            n1=self.grid_shape[0], n2=self.grid_shape[1], n3=self.grid_shape[2], nk=1,
+            npw=npw.ctypes.data_as(ct.POINTER(ct.c_int32)), miller=miller.ctypes.data_as(ct.POINTER(ct.c_int32)),
+            kinetic=kinetic.ctypes.data_as(ct.POINTER(ct.c_double)), nproj=0, projectors=None,
+            dij=dij.ctypes.data_as(ct.POINTER(ct.c_double)), nspin=1, precisions=1 << AMA_C128)
+        handle = ct.c_void_p()
+        with torch.cuda.device(self.device):
+            call("ama_engine_create", ct.byref(desc), ct.byref(handle))
+        self.handle = handle
+        self._lib = lib
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            try:
+                self._lib.ama_engine_destroy(h)
+            except Exception:  # pragma: no cover - interpreter shutdown
+                pass
+            self.handle = None
+
+
 def engine_for(system, precisions=("complex128", "complex64")) -> DeviceEngine:
     """The system's engine, created on first use and cached on the system object."""
     eng = getattr(system, "_device_engine", None)

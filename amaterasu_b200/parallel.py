@@ -1,7 +1,7 @@
 """k-point sharding of the SCF over GPUs (one process per GPU, torch.distributed).
 
 The Kohn-Sham problem is independent per (spin, k) inside an SCF iteration (amaterasu
-``scf/driver.py:442-460`` loops over them serially), so each rank takes a contiguous block
+``scf/driver.py:338-355`` loops over them serially), so each rank takes a contiguous block
 of k-points, balanced by its share of sum_k npw_k * nbands (the H.psi work). Per SCF
 iteration the ranks exchange:
 
@@ -12,8 +12,9 @@ iteration the ranks exchange:
 * the partial kinetic and nonlocal energies (one all-reduce of a few scalars).
 
 Everything else (potential, mixing, convergence test) is replicated and deterministic, so
-every rank takes the same collective steps in the same order. The backend is NCCL on GPUs
-and gloo for the CPU tests of this logic.
+every rank takes the same collective steps in the same order. The backend is NCCL on GPUs;
+with gloo (the CPU tests, and ranks sharing one GPU) device tensors are staged through host
+memory around each collective.
 """
 from __future__ import annotations
 
@@ -57,7 +58,12 @@ class KpointComm:
 
     def allreduce_(self, t: torch.Tensor) -> torch.Tensor:
         if self.world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.SUM, group=self.group)
+            if t.is_cuda and dist.get_backend(self.group) != "nccl":  # gloo reduces host tensors
+                host = t.cpu()
+                dist.all_reduce(host, op=dist.ReduceOp.SUM, group=self.group)
+                t.copy_(host)
+            else:
+                dist.all_reduce(t, op=dist.ReduceOp.SUM, group=self.group)
         return t
 
     def allreduce_scalars(self, values) -> np.ndarray:
@@ -94,7 +100,7 @@ def shard_system(system, parts, rank: int):
     from . import kpoints as kp
     k0, kc = parts[rank]
     local = copy.copy(system)
-    for attr in ("_device_engine", "_grid_ops", "_bd_cache", "_v_local_dev", "_sphere_tables"):
+    for attr in ("_device_engine", "_grid_ops", "_bd_cache", "_v_local_dev", "_sphere_tables", "_start_orbitals"):
         if hasattr(local, attr):
             delattr(local, attr)
     local.kpoints = kp.KPointSet(system.kpoints.points[k0:k0 + kc], system.kpoints.weights[k0:k0 + kc],

@@ -20,23 +20,26 @@ KERKER_SLOT = 1
 
 
 class GridOps:
-    """Grid-space FP64 operations of one system (cached on the system)."""
+    """Grid-space FP64 operations of one FFT grid: the Hartree filter (when the density
+    sphere is known), the Kerker filter and LDA-PZ. Cached on the system (and on its grid)
+    or, for a bare grid, on the grid object with an engine of its own."""
 
-    def __init__(self, system):
-        self.system = system
-        self.engine = engine_for(system)
+    def __init__(self, grid, engine, density_sphere=None):
+        self.grid = grid
+        self.engine = engine
         self.device = self.engine.device
-        grid = system.grid
         self.shape = tuple(int(n) for n in grid.shape)
         self.N = int(np.prod(self.shape))
-        self.dv = grid.cell_volume_per_point
-        self.volume = grid.volume
-        sphere = system.density_sphere
-        flat = grid.flat_indices(sphere)
-        f = np.zeros(self.N)
-        nz = sphere.g2 > 1e-12
-        f[flat[nz]] = 4.0 * np.pi / sphere.g2[nz]
-        call("ama_set_grid_filter", self.engine.handle, HARTREE_SLOT, f.ctypes.data_as(ct.c_void_p))
+        self.volume = abs(float(np.linalg.det(np.asarray(grid.cell, dtype=float))))
+        self.dv = self.volume / self.N
+        if density_sphere is not None:
+            sphere = density_sphere
+            h = np.stack([sphere.miller[:, a] % self.shape[a] for a in range(3)])
+            flat = ((h[0] * self.shape[1] + h[1]) * self.shape[2] + h[2]).astype(np.int64)
+            f = np.zeros(self.N)
+            nz = sphere.g2 > 1e-12
+            f[flat[nz]] = 4.0 * np.pi / sphere.g2[nz]
+            call("ama_set_grid_filter", self.engine.handle, HARTREE_SLOT, f.ctypes.data_as(ct.c_void_p))
         self._kerker_q0 = None
         self._energy = torch.zeros(1, dtype=torch.float64, device=self.device)
 
@@ -52,7 +55,7 @@ class GridOps:
     def set_kerker(self, q0: float, uniform_factor: float = 0.0):
         if self._kerker_q0 == (q0, uniform_factor):
             return
-        g = self.system.grid.gvectors_cartesian()
+        g = self.grid.gvectors_cartesian()
         g2 = np.einsum("...i,...i->...", g, g).ravel()
         with np.errstate(invalid="ignore", divide="ignore"):
             f = np.where(g2 > 1e-12, g2 / (g2 + q0**2), float(uniform_factor))
@@ -76,15 +79,33 @@ class GridOps:
         eps = torch.empty(self.N, dtype=torch.float64, device=self.device)
         vrho = torch.empty((2, self.N), dtype=torch.float64, device=self.device)
         call("ama_lda_pz", ptr(spin), self.N, ptr(eps), ptr(vrho), stream_ptr())
-        energy = (eps * (spin[0] + spin[1])).sum() * self.dv
-        return energy, vrho[:nspin]
+        total = d[0].contiguous() if nspin == 1 else (spin[0] + spin[1])
+        energy = torch.empty(1, dtype=torch.float64, device=self.device)
+        call("ama_vec_reduce", 0, self.N, ptr(eps), ptr(total), float(self.dv), 0, ptr(energy), stream_ptr())
+        return energy[0], vrho[:nspin]
 
 
 def grid_ops(system) -> GridOps:
     ops = getattr(system, "_grid_ops", None)
     if ops is None:
-        ops = GridOps(system)
+        ops = GridOps(system.grid, engine_for(system), system.density_sphere)
         system._grid_ops = ops
+        try:
+            system.grid._grid_ops = ops  # a mixer built from the bare grid reuses it
+        except AttributeError:  # pragma: no cover - frozen grid objects
+            pass
+    return ops
+
+
+def grid_ops_for_grid(grid) -> GridOps:
+    """GridOps of a bare FFT grid (ours or the reference's: anything with ``shape``, ``cell``
+    and ``gvectors_cartesian()``): the system's when the grid belongs to one, else one with a
+    minimal engine of its own (Kerker filtering only)."""
+    ops = getattr(grid, "_grid_ops", None)
+    if ops is None:
+        from .engine import GridEngine
+        ops = GridOps(grid, GridEngine(grid.shape))
+        grid._grid_ops = ops
     return ops
 
 

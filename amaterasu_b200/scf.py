@@ -1,12 +1,12 @@
 """The self-consistent field loop on the GPU (norm-conserving, symmetry off).
 
-Mirrors amaterasu ``scf/driver.py:372-569`` (``run_scf``, mixing branch): per iteration
+Mirrors amaterasu ``scf/driver.py:267-464`` (``run_scf``, mixing branch): per iteration
 v_eff[n_in] (Hartree + LDA + local), Davidson at every (spin, k) with the tolerance
 schedule clip(1e-3 min(residual, 1), 1e-11, 1e-6) and 40/20 iterations, occupations,
 n_out, the Kohn-Sham energy at n_out, the eigenvalue-sum identity, the density residual
 integral |n_out - n_in| / N_e, convergence when |dF| < tol_energy * natoms (eV -> Ha) and
 the residual < tol_density (from the second iteration on), then mixing. Starting
-orbitals are random_bands seeded 12345 + 991 spin + ik (driver.py:360-369).
+orbitals are random_bands seeded 12345 + 991 spin + ik (driver.py:255-264).
 
 Precision policy (``config.engine.precision``): "complex128" is the plain FP64 engine;
 "mixed" runs H.psi, Davidson and the density in complex64 and switches the orbitals to
@@ -31,7 +31,9 @@ from .batched import BatchedDavidson
 from .config import Config, parse_energy
 from .density import accumulate_packed, band_weights, finalize_density
 from .eigen import davidson, random_bands
-from .engine import check_device_status, engine_for, require_cuda
+from ._lib import call
+from .engine import check_device_status, engine_for, precision_code, ptr, require_cuda, stream_ptr
+from .linalg import gemm_nn
 from .hamiltonian import Hamiltonian
 from .mixing import create_mixer
 from .occupations import compute_occupations
@@ -120,7 +122,8 @@ def starting_orbitals(system, spin: int, ik: int) -> torch.Tensor:
     block = cache.get(key)
     if block is None:
         sphere = system.wave_spheres[ik]
-        block = random_bands(len(sphere), system.nbands, sphere.kinetic_energy, seed=12345 + 991 * spin + ik,
+        k_global = ik + (system.kparts[system.krank][0] if hasattr(system, "kparts") else 0)  # a rank's shard
+        block = random_bands(len(sphere), system.nbands, sphere.kinetic_energy, seed=12345 + 991 * spin + k_global,
                              dtype=torch.complex128)
         cache[key] = block
     return block
@@ -133,32 +136,57 @@ def prepare_starting_orbitals(system) -> None:
             starting_orbitals(system, spin, ik)
 
 
-def _kinetic_energy(system, orb: _Orbitals, occ, kin_dev) -> float:
-    """Local (this rank's k-points) kinetic energy; occ holds this rank's k-points."""
+def _band_factors(system, occ, spin) -> torch.Tensor:
     g = 2.0 / system.nspin
-    total = torch.zeros((), dtype=torch.float64, device=orb.packed[0].device)
+    w = g * np.asarray(system.kpoints.weights)[:, None] * np.asarray(occ)[spin]
+    return torch.from_numpy(np.ascontiguousarray(w.ravel(), dtype=np.float64))
+
+
+def _weighted_sum(rows: torch.Tensor, weights: torch.Tensor, acc: torch.Tensor, accumulate: bool) -> None:
+    call("ama_vec_reduce", 0, rows.numel(), ptr(rows), ptr(weights.to(rows.device)), 1.0, int(accumulate), ptr(acc),
+         stream_ptr())
+
+
+def _kinetic_energy(system, orb: _Orbitals, occ, kin_packed) -> float:
+    """Local (this rank's k-points) kinetic energy: per-band sum_G |psi|^2 T_G on the device
+    (``ama_band_kinetic``), weighted by 2/nspin w_k f_nk; occ holds this rank's k-points."""
+    eng = orb.eng
+    dev = orb.packed[0].device
+    rows = torch.empty(eng.nk * orb.nbands, dtype=torch.float64, device=dev)
+    acc = torch.zeros(1, dtype=torch.float64, device=dev)
+    npw = torch.from_numpy(eng.npw.astype(np.int32)).to(dev)
+    pw_off = torch.from_numpy(eng.pw_off[:-1].astype(np.int64)).to(dev)
     for spin in range(system.nspin):
-        for ik in range(system.nkpoints):
-            x = orb.block(spin, ik)
-            per_band = (x.real.double() ** 2 + x.imag.double() ** 2) @ kin_dev[ik]
-            f = torch.from_numpy(g * system.kpoints.weights[ik] * occ[spin, ik]).to(per_band.device)
-            total = total + (f * per_band).sum()
-    return float(total)
+        call("ama_band_kinetic", precision_code(orb.dtype), eng.nk, orb.nbands, ptr(npw), ptr(pw_off),
+             ptr(orb.packed[spin]), ptr(kin_packed), ptr(rows), stream_ptr())
+        _weighted_sum(rows, _band_factors(system, occ, spin), acc, spin > 0)
+    return float(acc[0])
 
 
 def _nonlocal_energy(system, orb: _Orbitals, occ, dij_dev) -> float:
+    """sum over bands of f <beta|psi>^* D <beta|psi>: the projections of each k (engine GEMM),
+    P D on the FP64 GEMM, and the per-band quadratic forms (``ama_rowdot``)."""
     eng = orb.eng
     if eng.nproj == 0:
         return 0.0
-    g = 2.0 / system.nspin
-    total = torch.zeros((), dtype=torch.float64, device=orb.packed[0].device)
+    dev = orb.packed[0].device
+    nb = orb.nbands
+    rows = torch.empty(eng.nk * nb, dtype=torch.float64, device=dev)
+    acc = torch.zeros(1, dtype=torch.float64, device=dev)
     for spin in range(system.nspin):
         for ik in range(system.nkpoints):
-            p = eng.project(orb.block(spin, ik), ik).to(torch.complex128)
-            quad = torch.einsum("ni,ij,nj->n", p.conj(), dij_dev, p).real
-            f = torch.from_numpy(g * system.kpoints.weights[ik] * occ[spin, ik]).to(quad.device)
-            total = total + (f * quad).sum()
-    return float(total)
+            p = eng.project(orb.block(spin, ik), ik).to(torch.complex128).contiguous()
+            q = gemm_nn(p, dij_dev)
+            call("ama_rowdot", nb, eng.nproj, ptr(p), ptr(q), ptr(rows[ik * nb:(ik + 1) * nb]), stream_ptr())
+        _weighted_sum(rows, _band_factors(system, occ, spin), acc, spin > 0)
+    return float(acc[0])
+
+
+def _grid_dot(a: torch.Tensor, b: torch.Tensor, op: int = 0) -> float:
+    """sum a*b (op 0) or sum |a - b| (op 1) over flat FP64 device vectors."""
+    out = torch.empty(1, dtype=torch.float64, device=a.device)
+    call("ama_vec_reduce", op, a.numel(), ptr(a.contiguous()), ptr(b.contiguous()), 1.0, 0, ptr(out), stream_ptr())
+    return float(out[0])
 
 
 def _density_out(system, orb: _Orbitals, occ, comm=None) -> torch.Tensor:
@@ -213,9 +241,10 @@ def run_scf(system, config: Config | None = None, *, logger=None, wavefunctions=
                 orb.set(spin, ik, starting_orbitals(system, spin, ik).to(wdtype))
     eng.reserve("complex128" if wdtype == torch.complex128 else "complex64", nb)
     kin_dev = [torch.from_numpy(s.kinetic_energy).to(dev) for s in system.wave_spheres]
+    kin_packed = torch.cat(kin_dev).contiguous()
     dij_dev = torch.from_numpy(system.projectors[0].dij).to(dev, torch.complex128) if eng.nproj else None
     vloc = torch.from_numpy(system.v_local.ravel()).to(dev)
-    mixer = create_mixer(config.scf.mixing, system)
+    mixer = create_mixer(config.scf.mixing, system.grid)
 
     threshold = config.scf.tol_energy * natoms * EV_IN_HARTREE
     history, trace, step_times = [], [], []
@@ -235,7 +264,7 @@ def run_scf(system, config: Config | None = None, *, logger=None, wavefunctions=
         if policy == "mixed" and orb.dtype == torch.complex64 and (residual < config.engine.refine_below or stalled):
             # the complex64 fixed point differs from the FP64 one by the FP32 rounding floor:
             # restart the mixer so that its history does not pull towards the former
-            mixer = create_mixer(config.scf.mixing, system)
+            mixer = create_mixer(config.scf.mixing, system.grid)
             orb.to(torch.complex128)
             eng.reserve("complex128", nb)
         prec_name = "complex64" if orb.dtype == torch.complex64 else "complex128"
@@ -290,20 +319,20 @@ def run_scf(system, config: Config | None = None, *, logger=None, wavefunctions=
         if system.core_density is not None:
             xc_d = rho_out + torch.from_numpy(system.core_density.ravel()).to(dev)[None] / system.nspin
         e_xc, _ = ops.lda(xc_d)
-        e_kin = _kinetic_energy(system, orb, occ, kin_dev)
+        e_kin = _kinetic_energy(system, orb, occ, kin_packed)
         e_nl = _nonlocal_energy(system, orb, occ, dij_dev)
         if distributed:
             e_kin, e_nl = comm.allreduce_scalars([e_kin, e_nl])
         energies = Energies(
             kinetic=float(e_kin),
-            local=float((vloc * rho_out.sum(0)).sum()) * dv,
+            local=_grid_dot(vloc, rho_out[0] if system.nspin == 1 else rho_out.sum(0)) * dv,
             hartree=float(e_h), xc=float(e_xc),
             nonlocal_=float(e_nl),
             ewald=system.ewald, entropy=occ_result.entropy_term)
         band_sum = 2.0 / system.nspin * float(np.einsum("k,skn,skn->", weights_all, occ_all, eig_all))
-        local_e = float((veff.reshape(system.nspin, -1) * rho_out).sum()) * dv
+        local_e = _grid_dot(veff.reshape(-1), rho_out.reshape(-1)) * dv
         identity = band_sum - (energies.kinetic + local_e + energies.nonlocal_)
-        residual = float((rho_out - rho_in).abs().sum()) * dv / system.nelectrons
+        residual = _grid_dot(rho_out.reshape(-1), rho_in.reshape(-1), op=1) * dv / system.nelectrons
         if orb.dtype == torch.complex64:
             res64.append(residual)
         energy = energies.free_energy

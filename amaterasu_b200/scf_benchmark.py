@@ -65,7 +65,9 @@ TRAINING_SPACING_A = 5.43 / 36  # working-grid spacing the committed nets were t
 
 
 def run(workload: str, weights=None, forces=False, log=print, policies=("plain", "mixed", "learned+mixed"),
-        engine_options=None, spacing=TRAINING_SPACING_A, stress=False) -> dict:
+        engine_options=None, spacing=TRAINING_SPACING_A, stress=False, hook=None) -> dict:
+    """Run the policies on one system; ``hook(name, "start"|"stop")`` brackets each timed run
+    (the bench samples clocks there)."""
     import torch
     from .learned import DensityNet, LearnedStart, working_grid
     from .scf import prepare_starting_orbitals, run_scf
@@ -83,12 +85,16 @@ def run(workload: str, weights=None, forces=False, log=print, policies=("plain",
     out = dict(workload=workload, setup_seconds=setup, natoms=system.natoms, runs={})
     results = {}
     for name, precision, start in runs:
+        if hook:
+            hook(name, "start")
         torch.cuda.synchronize()
         t = time.perf_counter()
         density = start.predict(system) if start is not None else None
         res = run_scf(system, _config(workload, precision, engine_options), density=density)
         torch.cuda.synchronize()
         seconds = time.perf_counter() - t
+        if hook:
+            hook(name, "stop")
         row = dict(seconds=seconds, iterations=res.iterations, converged=res.converged,
                    free_energy=res.energies.free_energy, precision_trace=res.precision_trace.count("complex64"))
         if start is not None:

@@ -69,10 +69,18 @@ class PlaneWaveSystem:
     nspin: int
     nbands: int
     nelectrons: float
-    ewald: float
     v_local: np.ndarray
     core_density: np.ndarray | None = None
     warnings: list = field(default_factory=list)
+    _ewald: float | None = field(default=None, repr=False)
+
+    @property
+    def ewald(self) -> float:
+        """Ion-ion Ewald energy (Ha), summed on the GPU the first time it is needed."""
+        if self._ewald is None:
+            charges = np.array([self.pseudopotentials[s].valence_charge for s in self.symbols])
+            self._ewald = float(ewald_energy(self.cell, self.positions, charges))
+        return self._ewald
 
     @property
     def volume(self) -> float:
@@ -134,13 +142,11 @@ def build_system(atoms, pseudopotentials: dict, ecut: float, ecut_rho: float | N
     else:
         projectors = [None] * len(wave_spheres)
     v_local = local_potential(grid, density_sphere, positions, symbols, pseudopotentials)
-    charges = np.array([pseudopotentials[s].valence_charge for s in symbols])
-    ewald = ewald_energy(cell, positions, charges)
     core = atomic_core_density(grid, density_sphere, positions, symbols, pseudopotentials)
     return PlaneWaveSystem(
         cell=cell, positions=positions, symbols=symbols, pseudopotentials=pseudopotentials, xc=xc,
         ecut=float(ecut), ecut_rho=float(ecut_rho), grid=grid, density_sphere=density_sphere,
         kpoints=kpoints, wave_spheres=wave_spheres, projectors=projectors, nspin=nspin,
-        nbands=int(nbands), nelectrons=float(nelectrons), ewald=float(ewald), v_local=v_local,
+        nbands=int(nbands), nelectrons=float(nelectrons), v_local=v_local,
         core_density=core, warnings=warnings,
     )

@@ -186,9 +186,12 @@ AMA_API int ama_grid_filter(AmaEngine* engine, int32_t slot, int32_t energy_slot
  * must not take cudaMalloc's device-wide synchronisation). No counterpart in the
  * reference. Same arguments and result as ama_grid_filter; the complex work grid is a
  * fixed device array of 128^3 points (32 MiB, held on every GPU that loads the library),
- * and a larger grid returns AMA_ERR_SHAPE. The first call on a device looks up the
- * array's address and should come before any stream capture. All calls share the array:
- * calls that overlap on the GPU race. */
+ * and a larger grid returns AMA_ERR_SHAPE. The array's address is looked up when an
+ * engine is created on the device (which also loads the library's device code there, so
+ * create the engine before a framework allocator reserves the GPU); that lookup happens
+ * before any stream capture the caller makes. The library does not survive a
+ * cudaDeviceReset of a device it has used. All calls share the array: calls that overlap
+ * on the GPU race. */
 AMA_API int ama_grid_filter_noalloc(AmaEngine* engine, int32_t slot, int32_t energy_slot,
                                     const double* in, double* out, double* energy, void* stream);
 
@@ -217,6 +220,56 @@ AMA_API int ama_kbatch_copy_rows(int32_t precision, int32_t nk, int32_t nrows, c
  * Replaces lda.exchange + lda.correlation_pz81 (xc/lda.py:122-142,203-262). */
 AMA_API int ama_lda_pz(const double* rho, int64_t npoints, double* eps, double* vrho, void* stream);
 
+/* ---- FP64 grid vectors of the SCF loop (mixers, density, energies). Vectors are device
+ * arrays of n doubles; `vectors` is a HOST array of nvec device pointers; coefficients are
+ * host arrays. Every reduction is deterministic (fixed summation order). */
+
+/* Overlaps of linear combinations of up to 16 vectors: u_a = sum_j coef[a*nvec+j] v_j for
+ * a < ncomb, plus u_ncomb = extra when extra != NULL; gram (device, (ncomb+e)^2 doubles,
+ * row-major, symmetric) = u_a . u_b. Replaces the residual overlap products of
+ * PulayMixer._coefficients and BroydenMixer (scf/mixing.py:173-193,238-258). */
+AMA_API int ama_vec_gram(int32_t nvec, const double* const* vectors, int32_t ncomb, const double* coef,
+                         const double* extra, int64_t n, double* gram, void* stream);
+
+/* out = sum_j coef[j] v_j (up to 16 vectors). Replaces the history combinations of the
+ * mixers (scf/mixing.py:195-201, 258-260). */
+AMA_API int ama_vec_lincomb(int32_t nvec, const double* const* vectors, const double* coef, int64_t n,
+                            double* out, void* stream);
+
+/* *out = (accumulate ? *out : 0) + scale * R with R = sum a*b (op 0), sum |a - b| (op 1),
+ * sum a (op 2) or sum max(a, 0) (op 3); out is a device double. The energy integrals and the
+ * density residual of run_scf (scf/driver.py:376-419). */
+AMA_API int ama_vec_reduce(int32_t op, int64_t n, const double* a, const double* b, double scale,
+                           int32_t accumulate, double* out, void* stream);
+
+/* rho[c] <- max(rho[c] / volume, 0) * (sum rho[c] / sum max(rho[c], 0)) for each of the
+ * nchannels channels of n points (in place): the 1/Omega and the charge-preserving floor of
+ * compute_density (scf/density.py:71-84, symmetry off). */
+AMA_API int ama_density_floor(int32_t nchannels, int64_t n, double volume, double* rho, void* stream);
+
+/* rows[k*nbands + b] = sum_G |psi_bk(G)|^2 T_k(G) over the packed per-k blocks (npw, pw_off
+ * device as for ama_kbatch_zgemm, kinetic packed by pw_off). Per-band kinetic energies of
+ * _kinetic_energy (scf/driver.py:520-528). */
+AMA_API int ama_band_kinetic(int32_t precision, int32_t nk, int32_t nbands, const int32_t* npw,
+                             const int64_t* pw_off, const void* psi, const double* kinetic, double* rows,
+                             void* stream);
+
+/* rows[i] = Re sum_j conj(a[i][j]) b[i][j] for complex128 row-major (nrows, ncols) arrays:
+ * the per-band <beta|psi>^* D <beta|psi> of _nonlocal_energy (scf/driver.py:531-541). */
+AMA_API int ama_rowdot(int32_t nrows, int32_t ncols, const void* a, const void* b, double* rows, void* stream);
+
+/* Ewald energy, forces and stress of point charges in a periodic cell (FP64):
+ *   out[0] = E (Ha); out[1 + 3a + c] = F_a,c (Ha/Bohr); out[1 + 3 natoms + 3i + j] = sigma_ij
+ *   = (1/Omega) dE/d eps_ij (Ha/Bohr^3).
+ * positions [natoms][3] Bohr, charges [natoms], shifts [nshift][3] lattice translations
+ * covering the real-space cutoff rcut (terms with r > rcut are skipped), gvectors [ng][3]
+ * nonzero reciprocal vectors of the reciprocal sum, eta the splitting parameter, volume the
+ * cell volume; work holds 13 natoms + 9 ng doubles, 16-byte aligned. All arrays on the device. Replaces
+ * hamiltonian/ewald.py:94-228 (ewald). */
+AMA_API int ama_ewald(int32_t natoms, const double* positions, const double* charges, const double* shifts,
+                      int32_t nshift, const double* gvectors, int32_t ng, double eta, double rcut, double volume,
+                      double* work, double* out, void* stream);
+
 /* Structure sums of the set-up (superposed atomic densities and local potentials):
  *   out[g] = scale * sum_a radial[species[a] * ng + g] * exp(-i G_g . tau_a)
  * gcart: device FP64 [ng][3] Cartesian G vectors; positions: [natoms][3] Bohr; species:
@@ -225,7 +278,7 @@ AMA_API int ama_lda_pz(const double* rho, int64_t npoints, double* eps, double* 
 AMA_API int ama_structure_sum(const double* gcart, int32_t ng, const double* positions, const int32_t* species,
                               int32_t natoms, const double* radial, double scale, double* out, void* stream);
 
-/* Dense FP64 Hermitian eigensolver for `batch` matrices of order n <= 3456 (device,
+/* Dense FP64 Hermitian eigensolver for `batch` matrices of order n <= 2400 (device,
  * row-major, interleaved complex, overwritten by eigenvectors as columns); eigenvalues
  * ascending. Hand-written: Householder tridiagonalisation in one cooperative launch,
  * multisection bisection, inverse iteration with Gram-Schmidt inside eigenvalue clusters,

@@ -2,7 +2,7 @@
 
 Follows amaterasu ``scf/density.py:35-84``, ``scf/occupations.py:38-244`` (Fermi-Dirac,
 Gaussian, Methfessel-Paxton, Marzari-Vanderbilt, fixed), ``scf/mixing.py:48-285``
-(Kerker, linear, Pulay, Anderson, Broyden) and ``scf/driver.py:372-569`` (run_scf, NC
+(Kerker, linear, Pulay, Anderson, Broyden) and ``scf/driver.py:267-464`` (run_scf, NC
 branch, symmetry off).
 """
 from __future__ import annotations

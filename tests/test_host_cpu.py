@@ -49,3 +49,50 @@ def test_device_timeout_is_raised_not_ignored(monkeypatch):
     words.update(ama_tc_status=0, ama_solver_status=1)
     with pytest.raises(E.DeviceTimeout, match="eigensolver"):
         E.check_device_status(FakeEngine())
+
+
+@pytest.mark.parametrize("scheme", ["fermi-dirac", "gaussian", "methfessel-paxton", "marzari-vanderbilt"])
+@pytest.mark.parametrize("order", [1, 2, 3])
+def test_smearing_functions_match_the_oracle(scheme, order):
+    """The published closed forms (Methfessel-Paxton's A_n H_{2n-1} sum and A_N H_2N entropy,
+    Marzari-Vanderbilt, a log-free Fermi-Dirac entropy) against the oracle's restatement of
+    the reference's recursions, to 1e-14."""
+    import numpy as np
+    from amaterasu_b200 import occupations as occ
+    from oracle import scf as o
+    x = np.linspace(-12.0, 12.0, 2001)
+    np.testing.assert_allclose(occ.occupation_function(x, scheme, order), o.occupation_function(x, scheme, order),
+                               rtol=0, atol=1e-14)
+    np.testing.assert_allclose(occ.entropy_function(x, scheme, order), o.entropy_function(x, scheme, order),
+                               rtol=0, atol=1e-14)
+
+
+@pytest.mark.parametrize("scheme,smearing", [("gaussian", 0.01), ("fermi-dirac", 0.005), ("methfessel-paxton", 0.02),
+                                             ("marzari-vanderbilt", 0.02), ("fixed", 0.0)])
+def test_occupations_match_the_oracle(scheme, smearing):
+    import numpy as np
+    from amaterasu_b200.occupations import compute_occupations
+    from oracle.scf import compute_occupations as oracle_occupations
+    rng = np.random.default_rng(4)
+    eig = np.sort(rng.uniform(-0.3, 0.6, size=(1, 7, 12)), axis=2)
+    w = rng.uniform(0.5, 1.5, 7)
+    w /= w.sum()
+    res = compute_occupations(eig, w, 13.0, scheme=scheme, smearing=smearing)
+    occ, fermi, ent, gap = oracle_occupations(eig, w, 13.0, scheme, smearing)
+    np.testing.assert_allclose(res.occupations, occ, rtol=0, atol=1e-11)
+    np.testing.assert_allclose(res.fermi_level, fermi, rtol=0, atol=1e-11)
+    np.testing.assert_allclose(res.entropy_term, ent, rtol=0, atol=1e-12)
+
+
+def test_occupations_match_reference_golden(mini_system):
+    import numpy as np
+    from conftest import golden
+    from amaterasu_b200.occupations import compute_occupations
+    g = golden("mini.npz")
+    eig = np.array([[g["dav_eig0"], g["dav_eig1"]]])
+    res = compute_occupations(eig, mini_system.kpoints.weights, mini_system.nelectrons, scheme="gaussian",
+                              smearing=0.1 / 27.211386, nspin=1)
+    np.testing.assert_allclose(res.occupations, g["occ"], rtol=0, atol=1e-12)
+    np.testing.assert_allclose(res.fermi_level, float(g["fermi"]), rtol=0, atol=1e-11)
+    with pytest.raises(ValueError, match="not one of"):
+        compute_occupations(eig, mini_system.kpoints.weights, 8.0, scheme="bogus", smearing=0.01)

@@ -40,6 +40,39 @@ def test_noalloc_filter_matches_allocating_filter(mini_system):
         assert abs(e_got - e_ref) <= 1e-12 * abs(e_ref)
 
 
+def test_noalloc_filter_without_energy_allocates_nothing(si_pseudo):
+    """energy_slot -1 with no energy pointer (the Kerker use), on a fresh engine whose grid
+    differs from the allocating path's last one: same result as ama_grid_filter, and the
+    device's free memory does not move across further calls (the call allocates nothing)."""
+    from amaterasu_b200 import _lib
+    from amaterasu_b200 import kpoints as kp
+    from amaterasu_b200.cells import si2_primitive
+    from amaterasu_b200.engine import ptr, stream_ptr
+    from amaterasu_b200.potential import grid_ops
+    from amaterasu_b200.system import build_system
+    lib = _lib.load()
+    s = build_system(si2_primitive(), {"Si": si_pseudo}, 6.0, 24.0, kpoints=kp.gamma_only(), nbands=4)
+    ops = grid_ops(s)
+    ops.set_kerker(1.5)  # slot 1
+    handle = ops.engine.handle
+    n = int(np.prod(s.grid.shape))
+    rho = torch.from_numpy(np.random.default_rng(7).normal(size=n)).cuda()
+    ref = torch.empty_like(rho)
+    assert lib.ama_grid_filter(handle, 1, -1, ptr(rho), ptr(ref), None, stream_ptr()) == 0
+    out = torch.empty_like(rho)
+    assert lib.ama_grid_filter_noalloc(handle, 1, -1, ptr(rho), ptr(out), None, stream_ptr()) == 0
+    torch.cuda.synchronize()
+    scale = float(ref.abs().max())
+    assert float((out - ref).abs().max()) <= 1e-12 * scale
+    free_before, _ = torch.cuda.mem_get_info()
+    for _ in range(3):
+        assert lib.ama_grid_filter_noalloc(handle, 1, -1, ptr(rho), ptr(out), None, stream_ptr()) == 0
+    torch.cuda.synchronize()
+    free_after, _ = torch.cuda.mem_get_info()
+    assert free_after == free_before
+    assert float((out - ref).abs().max()) <= 1e-12 * scale
+
+
 def test_noalloc_filter_rejects_grids_beyond_its_array():
     from amaterasu_b200 import _lib
     lib = _lib.load()
