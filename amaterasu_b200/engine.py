@@ -44,6 +44,34 @@ def ptr(t: torch.Tensor) -> ct.c_void_p:
     return ct.c_void_p(t.data_ptr())
 
 
+def system_tables(system) -> dict:
+    """The host arrays of an ``AmaSystemDesc`` for a plane-wave system: grid shape, plane
+    waves per k, Miller indices (sphere order, k-major), kinetic energies, projector
+    matrices (k-major, row-major (nproj, npw_k)) and D. Works on this package's
+    ``PlaneWaveSystem`` and on the reference's (amaterasu ``hamiltonian/system.py:71-122``):
+    both expose ``grid.shape``, ``wave_spheres[k].miller / .kinetic_energy``,
+    ``projectors[k].matrix / .dij`` and ``nspin``."""
+    spheres = system.wave_spheres
+    projs = system.projectors
+    nproj = 0 if projs[0] is None else int(np.asarray(projs[0].matrix).shape[0])
+    tables = {
+        "grid": tuple(int(n) for n in system.grid.shape),
+        "npw": np.array([len(s.miller) for s in spheres], dtype=np.int32),
+        "miller": np.ascontiguousarray(np.concatenate([s.miller for s in spheres]).astype(np.int32)),
+        "kinetic": np.ascontiguousarray(np.concatenate([s.kinetic_energy for s in spheres]), dtype=np.float64),
+        "nproj": nproj,
+        "nspin": int(system.nspin),
+    }
+    if nproj:
+        tables["projectors"] = np.ascontiguousarray(
+            np.concatenate([np.asarray(p.matrix, dtype=np.complex128).ravel() for p in projs])).view(np.float64)
+        tables["dij"] = np.ascontiguousarray(projs[0].dij, dtype=np.float64)
+    else:
+        tables["projectors"] = np.zeros(2)
+        tables["dij"] = np.zeros(1)
+    return tables
+
+
 class DeviceEngine:
     """The C-ABI engine of a system, plus per-k offsets for packed band blocks."""
 
@@ -52,25 +80,18 @@ class DeviceEngine:
         lib = _lib.load()
         self.system = system
         spheres = system.wave_spheres
-        self.npw = np.array([len(s) for s in spheres], dtype=np.int32)
+        t = system_tables(system)
+        self.npw = t["npw"]
         self.pw_off = np.concatenate([[0], np.cumsum(self.npw.astype(np.int64))])
         self.nk = len(spheres)
-        self.grid_shape = tuple(int(n) for n in system.grid.shape)
+        self.grid_shape = t["grid"]
         self.N = int(np.prod(self.grid_shape))
-        self.nspin = system.nspin
-        miller = np.ascontiguousarray(np.concatenate([s.miller for s in spheres]).astype(np.int32))
-        kinetic = np.ascontiguousarray(np.concatenate([s.kinetic_energy for s in spheres]), dtype=np.float64)
+        self.nspin = t["nspin"]
+        miller, kinetic = t["miller"], t["kinetic"]
         self.kinetic = [torch.from_numpy(np.ascontiguousarray(s.kinetic_energy)).to(self.device)
                         for s in spheres]
-        projs = system.projectors
-        self.nproj = 0 if projs[0] is None else len(projs[0])
-        if self.nproj:
-            pmat = np.ascontiguousarray(
-                np.concatenate([p.matrix.astype(np.complex128).ravel() for p in projs])).view(np.float64)
-            dij = np.ascontiguousarray(projs[0].dij, dtype=np.float64)
-        else:
-            pmat = np.zeros(2)
-            dij = np.zeros(1)
+        self.nproj = t["nproj"]
+        pmat, dij = t["projectors"], t["dij"]
         mask = 0
         for p in precisions:
             mask |= 1 << precision_code(p)
@@ -107,8 +128,9 @@ class DeviceEngine:
 
     def set_stage_b_variant(self, precision, variant: int) -> None:
         """Select the stage B kernel (x transforms and V): 0 shared-memory slabs, 1 register-
-        resident x columns, 2 register-resident with the compile-time x-plane set. Raises
-        NotImplementedError when the variant is not compiled for this grid."""
+        resident x columns, 2 register-resident with the compile-time x-plane set, 3 register-
+        resident with two threads per column. Raises NotImplementedError when the variant is
+        not compiled for this grid."""
         option = 1 if precision_code(precision) == AMA_C64 else 2
         call("ama_engine_option", self.handle, option, int(variant))
 

@@ -37,6 +37,24 @@ HERE = Path(__file__).resolve().parent
 REPO = HERE.parent.parent
 
 
+DEFAULT_REFERENCE = "/root/reference"
+
+
+def reference_mini_system():
+    """The reference's own PlaneWaveSystem for the mini configuration (Si2, two explicit
+    k-points, 8 Ha), or None when the reference is not at DEFAULT_REFERENCE."""
+    if not Path(DEFAULT_REFERENCE, "amaterasu").is_dir():
+        return None
+    _import_reference(DEFAULT_REFERENCE)
+    from amaterasu_b200.cells import si2_primitive
+    with tempfile.TemporaryDirectory() as tmp:
+        pseudo, _ = _upf(tmp)
+    kpts = [[0.0, 0.0, 0.0], [0.125, -0.25, 0.375]]
+    cfg = _config(kpoints__scheme="explicit", kpoints__points=kpts, occupations__nbands=6,
+                  occupations__scheme="gaussian", occupations__smearing=0.1)
+    return _system(si2_primitive(), cfg, pseudo, 8.0)
+
+
 def _import_reference(path: str):
     sys.path.insert(0, str(HERE / "shim"))
     sys.path.insert(0, path)
@@ -334,7 +352,7 @@ def make_si215(pseudo, out):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=DEFAULT_REFERENCE)
     ap.add_argument("--only", nargs="*", default=None)
     args = ap.parse_args()
     _import_reference(args.reference)

@@ -96,3 +96,59 @@ def test_occupations_match_reference_golden(mini_system):
     np.testing.assert_allclose(res.fermi_level, float(g["fermi"]), rtol=0, atol=1e-11)
     with pytest.raises(ValueError, match="not one of"):
         compute_occupations(eig, mini_system.kpoints.weights, 8.0, scheme="bogus", smearing=0.01)
+
+
+def test_engine_tables_from_a_reference_system(mini_system):
+    """The drop-in boundary with the reference's own objects: the AmaSystemDesc host tables
+    (grid, plane-wave counts, Miller indices in sphere order, kinetic energies, projector
+    matrices, D) that the engine builds from the reference's PlaneWaveSystem equal the ones
+    from this package's system, so Hamiltonian(reference_system, v_eff) sets up the same
+    engine. Needs the reference source tree (skipped where it is absent)."""
+    import sys
+
+    import numpy as np
+    from conftest import GOLDEN
+    sys.path.insert(0, str(GOLDEN))
+    import make_golden
+    from amaterasu_b200.engine import system_tables
+    ref_system = make_golden.reference_mini_system()
+    if ref_system is None:
+        pytest.skip("the reference source tree is not available here")
+    ours, theirs = system_tables(mini_system), system_tables(ref_system)
+    assert ours["grid"] == theirs["grid"] and ours["nproj"] == theirs["nproj"] and ours["nspin"] == theirs["nspin"]
+    np.testing.assert_array_equal(ours["npw"], theirs["npw"])
+    np.testing.assert_array_equal(ours["miller"], theirs["miller"])
+    np.testing.assert_allclose(ours["kinetic"], theirs["kinetic"], rtol=0, atol=1e-13)
+    np.testing.assert_allclose(ours["projectors"], theirs["projectors"], rtol=0, atol=1e-12)
+    np.testing.assert_array_equal(ours["dij"], theirs["dij"])
+
+
+def test_results_round_trip_in_output_units(tmp_path, mini_system):
+    """write_scf / read_scf: the reference's groups and output units (eV, Angstrom, eV/A,
+    eV/A^3 positive under compression), and the restart fields back in internal units."""
+    import numpy as np
+    from amaterasu_b200.results import read_scf, write_scf
+    from amaterasu_b200.scf import Energies, SCFResult
+    from amaterasu_b200.units import BOHR_IN_ANG, HARTREE_IN_EV
+    s = mini_system
+    rng = np.random.default_rng(0)
+    dens = np.abs(rng.normal(size=(1, *s.grid.shape)))
+    wfs = [[rng.normal(size=(6, len(w))) + 1j * rng.normal(size=(6, len(w))) for w in s.wave_spheres]]
+    res = SCFResult(converged=True, iterations=7, energies=Energies(kinetic=1.0, local=-2.0, hartree=0.5, xc=-0.7,
+                                                                    nonlocal_=0.3, ewald=-8.0, entropy=0.01),
+                    eigenvalues=rng.normal(size=(1, 2, 6)), occupations=rng.random((1, 2, 6)), fermi_level=0.2,
+                    gap=None, magnetization=0.0, density=dens, wavefunctions=wfs, history=[(1.0, 0.1, 0.0)],
+                    electron_count=8.0)
+    stress = np.diag([1e-4, 2e-4, 3e-4])
+    path = write_scf(tmp_path / "r.npz", s, res, forces=np.ones((2, 3)) * 1e-3, stress=stress,
+                     save_wavefunctions=True)
+    out = read_scf(path)
+    assert out["@format_version"] == 2 and out["@stress_convention"] == "positive_under_compression"
+    np.testing.assert_allclose(out["scf"]["energies"]["@free_energy"], res.energies.free_energy * HARTREE_IN_EV)
+    np.testing.assert_allclose(out["scf"]["eigenvalues"], res.eigenvalues * HARTREE_IN_EV)
+    np.testing.assert_allclose(out["structure"]["cell"], s.cell * BOHR_IN_ANG)
+    assert np.all(np.diag(out["stress"]) < 0)  # tensile internal stress is negative under compression
+    assert out["@pressure_GPa"] < 0
+    np.testing.assert_allclose(out["density_internal"], dens, rtol=1e-14)
+    for a, b in zip(out["wavefunctions"][0], wfs[0]):
+        np.testing.assert_array_equal(a, b)
