@@ -410,6 +410,72 @@ stage_b_sparse_kernel(HpsiView v, const float2* __restrict__ tw_xb, const float2
   });
 }
 
+// Stage B with two threads per (y, z) column (complex64, even compile-time n1 = 2 M): each
+// lane of an adjacent pair holds M of the n1 values, so the line never spills out of
+// registers. Backward transform by decimation in frequency index: lane h takes the inputs
+// G = 2m + h and transforms them with a length-M register DFT; the radix-2 combination
+// X[k + M j] = Y_0[k] + (-1)^j w^k Y_1[k] (w = e^{2 pi i / n1}) is done across the pair with
+// warp shuffles, lane h keeping the half j = h. The potential multiplies the natural x
+// index i = k + M h at the engine's permuted x position. The forward transform mirrors it:
+// Z_h[k] = (X[k] + (-1)^h X[k + M]) w^{-h k} across the pair, then a length-M DFT gives the
+// outputs G = 2m + h. Slots are looked up at run time; unused x-planes are neither read
+// nor written.
+template <int M, int AH>
+__host__ __device__ constexpr int half_index(int p) {  // index held at register p after the natural-in DFT
+  return p / (M / AH) + AH * (p % (M / AH));
+}
+
+template <int NX, int AH, class D>
+__global__ void __launch_bounds__(kRegBThreads)
+stage_b_pair_kernel(HpsiView v, const float2* __restrict__ tw_xb, const float2* __restrict__ tw_xf,
+                    const float* __restrict__ vpot, float2* __restrict__ work) {
+  constexpr int M = NX / 2;
+  AMA_DIMS(D, v)
+  const int gt = blockIdx.x * kRegBThreads + threadIdx.x;
+  const int col_raw = gt >> 1, h = gt & 1;
+  const bool live = col_raw < plane;  // both lanes of a pair agree
+  const int col = live ? col_raw : 0;  // dead pairs still take part in the shuffles
+  float2* wb = work + (int64_t)blockIdx.y * v.band_elems + col;
+  float2 r[M];
+  static_for<M>([&](auto mm) {
+    constexpr int m = decltype(mm)::value;
+    const int slot = live ? __ldg(v.slot_of_x + 2 * m + h) : -1;
+    r[m] = slot >= 0 ? wb[(int64_t)slot * plane] : make_float2(0.f, 0.f);
+  });
+  dft_line_reg<M, AH, +1, true>(r, tw_xb);
+  static_for<M>([&](auto pp) {
+    constexpr int p = decltype(pp)::value;
+    constexpr int k = half_index<M, AH>(p);
+    const float2 mine = r[p];
+    const float2 other = make_float2(__shfl_xor_sync(0xffffffffu, mine.x, 1), __shfl_xor_sync(0xffffffffu, mine.y, 1));
+    const float2 y0 = h ? other : mine;
+    const float2 t = line_twiddle<NX, +1, k>(h ? mine : other, tw_xb);
+    r[p] = h ? csub(y0, t) : cadd(y0, t);
+    const int i = k + M * h;                       // natural x index of the real-space value
+    const int pos = (i % A1) * B1 + i / A1;        // its position in the engine's permuted x order
+    const float sv = __ldg(vpot + (int64_t)pos * plane + col);
+    r[p].x *= sv;
+    r[p].y *= sv;
+  });
+  static_for<M>([&](auto pp) {
+    constexpr int p = decltype(pp)::value;
+    constexpr int k = half_index<M, AH>(p);
+    const float2 mine = r[p];
+    const float2 other = make_float2(__shfl_xor_sync(0xffffffffu, mine.x, 1), __shfl_xor_sync(0xffffffffu, mine.y, 1));
+    const float2 lo = h ? other : mine, hi = h ? mine : other;  // X[k], X[k + M]
+    const float2 z = h ? csub(lo, hi) : cadd(lo, hi);
+    const float2 zt = line_twiddle<NX, -1, k>(z, tw_xf);
+    r[p] = h ? zt : z;
+  });
+  dft_line_reg<M, AH, -1, false>(r, tw_xf);
+  if (!live) return;
+  static_for<M>([&](auto mm) {
+    constexpr int m = decltype(mm)::value;
+    const int slot = __ldg(v.slot_of_x + 2 * m + h);
+    if (slot >= 0) wb[(int64_t)slot * plane] = r[m];
+  });
+}
+
 template <typename T, class D>
 __global__ void __launch_bounds__(kFftThreads)
 stage_c_kernel(HpsiView v, const cx_t<T>* __restrict__ tw_y, const cx_t<T>* __restrict__ tw_z,
@@ -502,11 +568,12 @@ density_b_kernel(HpsiView v, const cx_t<T>* __restrict__ tw_xb, const cx_t<T>* _
 }
 
 // The stage B variants compiled for a grid: [0] shared-memory slab, [1] register-resident
-// x columns, [2] register-resident with the compile-time slot set (null when absent).
+// x columns, [2] register-resident with the compile-time slot set, [3] register-resident
+// with two threads per column (null when absent).
 struct StageInfo {
   int zsplit;
   bool regb;
-  const void* b_variant[3];
+  const void* b_variant[4];
 };
 
 template <typename T, class D>
@@ -521,12 +588,26 @@ StageInfo fill_stage_table(const void** fn) {
 // complex64 on a compile-time grid with short x columns: register-resident stage B
 // (register-resident y columns for stages A and C were measured slower than the
 // shared-memory passes at 84^3 and are not used)
+// the two-lanes-per-column stage B, when n1 is even and both line lengths have immediate
+// twiddles (the half-length DFT cannot take its twiddles from the n1 table)
+template <int N1, class D>
+void add_pair_variant(StageInfo& info) {
+  if constexpr (N1 % 2 == 0) {
+    constexpr int M = N1 / 2;
+    if constexpr (LineTwiddles<M>::kHave && LineTwiddles<N1>::kHave) {
+      constexpr int AH = M % 6 == 0 && M / 6 > 1 ? 6 : (M % 3 == 0 ? 3 : (M % 2 == 0 ? 2 : M));
+      info.b_variant[3] = (const void*)stage_b_pair_kernel<N1, AH, D>;
+    }
+  }
+}
+
 template <int N1, int A1, int N2, int A2, int N3, class D>
 StageInfo fill_stage_table_reg(const void** fn, int hp, int hn) {
   StageInfo info = fill_stage_table<float, D>(fn);
   fn[1] = (const void*)stage_b_reg_kernel<N1, A1, D>;
   info.regb = true;
   info.b_variant[1] = fn[1];
+  add_pair_variant<N1, D>(info);
   if constexpr (N1 == 84) {  // the Si64 benchmark grid: sparse-x variants for its slot sets
 #define AMA_SPARSE(P, Q) \
     if (hp == P && hn == Q) fn[1] = info.b_variant[2] = (const void*)stage_b_sparse_kernel<84, 12, P, Q, D>;
@@ -544,10 +625,15 @@ StageInfo select_stage_table(const AxisPlan* ax, const void** fn, int hp, int hn
   if (ax[0].n == N1 && ax[0].A == A1 && ax[1].n == N2 && ax[1].A == A2 && ax[2].n == N3 &&      \
       ax[2].A == A3) {                                                                           \
     using D = FixDims<N1, A1, N2, A2, N3, A3>;                                                   \
-    if constexpr (std::is_same<T, float>::value && N1 <= 96)                                     \
+    if constexpr (std::is_same<T, float>::value && N1 <= 96) {                                   \
       return fill_stage_table_reg<N1, A1, N2, A2, N3, D>(fn, hp, hn);                            \
-    else                                                                                         \
+    } else if constexpr (std::is_same<T, float>::value) { /* longer x lines: only two lanes */   \
+      StageInfo info = fill_stage_table<T, D>(fn);                                               \
+      add_pair_variant<N1, D>(info);                                                             \
+      return info;                                                                               \
+    } else {                                                                                     \
       return fill_stage_table<T, D>(fn);                                                         \
+    }                                                                                            \
   }
   AMA_FIX(20, 5, 20, 5, 20, 5)
   AMA_FIX(25, 5, 25, 5, 25, 5)
@@ -671,7 +757,8 @@ int set_smem_limits(const AmaEngine* e) {
   const StageInfo info = select_stage_table<T>(e->ax, fn, e->slot_hp, e->slot_hn);
   const_cast<AmaEngine*>(e)->zsplit[p] = info.zsplit;
   const_cast<AmaEngine*>(e)->regb[p] = info.regb;
-  for (int i = 0; i < 3; ++i) const_cast<AmaEngine*>(e)->b_variant[p][i] = info.b_variant[i];
+  const_cast<AmaEngine*>(e)->bthreads[p] = 1;
+  for (int i = 0; i < 4; ++i) const_cast<AmaEngine*>(e)->b_variant[p][i] = info.b_variant[i];
   AMA_CUDA_TRY(cudaFuncSetAttribute(fn[0], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
   AMA_CUDA_TRY(cudaFuncSetAttribute(fn[2], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
   AMA_CUDA_TRY(cudaFuncSetAttribute(info.b_variant[0], cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -727,7 +814,7 @@ int hpsi_impl(AmaEngine* e, int k_first, int k_count, int nbands, int spin, cons
   rc = run_fft_stages_a<T>(e, v, (int)nb_total, psi, s);
   if (rc) return rc;
   if (e->regb[p]) {
-    dim3 gr((e->ax[1].n * e->ax[2].n + kRegBThreads - 1) / kRegBThreads, nb_total);
+    dim3 gr((e->ax[1].n * e->ax[2].n * e->bthreads[p] + kRegBThreads - 1) / kRegBThreads, nb_total);
     ((StageBFn<T>)e->stage_fn[p][1])<<<gr, kRegBThreads, 0, s>>>(
         v, (const C*)e->d.tw[p][0][0], (const C*)e->d.tw[p][0][1], vpot, (C*)e->work[p]);
   } else {
@@ -1358,15 +1445,17 @@ extern "C" int ama_engine_option(AmaEngine* e, int32_t option, int32_t value) {
     case 0:  // nonlocal products of the complex64 path on the tensor cores (1) or SIMT (0)
       e->use_tc = value != 0;
       return AMA_OK;
-    case 1:  // complex64 stage B variant: 0 shared memory, 1 register, 2 register + slot set
+    case 1:  // complex64 stage B variant: 0 shared memory, 1 register, 2 register + slot set,
+             // 3 register, two threads per column
     case 2: {  // complex128 stage B variant (only 0 is compiled)
       const int p = option == 1 ? AMA_C64 : AMA_C128;
       AMA_REQUIRE(e->precisions & (1u << p), AMA_ERR_ARG, "the engine was created without this precision");
-      AMA_REQUIRE(value >= 0 && value < 3, AMA_ERR_ARG, "stage B variant must be 0, 1 or 2");
+      AMA_REQUIRE(value >= 0 && value < 4, AMA_ERR_ARG, "stage B variant must be 0, 1, 2 or 3");
       AMA_REQUIRE(e->b_variant[p][value] != nullptr, AMA_ERR_UNSUPPORTED,
                   "this stage B variant is not compiled for the engine's grid");
       e->stage_fn[p][1] = e->b_variant[p][value];
       e->regb[p] = value != 0;
+      e->bthreads[p] = value == 3 ? 2 : 1;
       return AMA_OK;
     }
     default:

@@ -76,7 +76,8 @@ struct AmaEngine {
   const void* stage_fn[2][4] = {};  // [prec][stage A, B, C, density B] (grid-specialised)
   int zsplit[2] = {1, 1};           // [prec] z halves per stage-B slab
   bool regb[2] = {false, false};    // [prec] stage B with register-resident x columns
-  const void* b_variant[2][3] = {};  // [prec] stage B variants compiled for the grid
+  const void* b_variant[2][4] = {};  // [prec] stage B variants compiled for the grid
+  int bthreads[2] = {1, 1};          // [prec] threads per (y, z) column of the register stage B
   NlTcState tc;
   bool use_tc = true;
   // FP64 grid transforms (Hartree, Kerker): reciprocal-space filters in the engine's

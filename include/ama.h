@@ -71,7 +71,8 @@ AMA_API int ama_engine_destroy(AmaEngine* engine);
  *             or on the SIMT GEMM (value 0);
  *   option 1: complex64 stage B (x transforms and V) variant: 0 shared-memory slabs,
  *             1 register-resident x columns, 2 register-resident with the spheres' compile-time
- *             x-plane set; AMA_ERR_UNSUPPORTED when the variant is not compiled for the grid;
+ *             x-plane set, 3 register-resident with two threads per column (even x length);
+ *             AMA_ERR_UNSUPPORTED when the variant is not compiled for the grid;
  *   option 2: the same for complex128 (only variant 0 exists).
  * amaterasu_b200.autotune times the variants and keeps the fastest. */
 AMA_API int ama_engine_option(AmaEngine* engine, int32_t option, int32_t value);

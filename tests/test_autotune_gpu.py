@@ -18,7 +18,7 @@ def _rel(a, b):
 
 def _available(eng, precision):
     out = []
-    for v in (0, 1, 2):
+    for v in (0, 1, 2, 3):
         try:
             eng.set_stage_b_variant(precision, v)
             out.append(v)
@@ -55,7 +55,8 @@ def test_every_variant_matches_the_oracle(mini_system, precision, tol):
 
 
 def test_si64_variants_match_the_reference(si_pseudo):
-    """84^3 grid: shared-memory, register and sparse register stage B against the golden."""
+    """84^3 grid: shared-memory, register, sparse register and two-lane register stage B
+    against the golden."""
     from amaterasu_b200.autotune import autotune_hpsi
     from amaterasu_b200.cells import workload
     from amaterasu_b200.hamiltonian import Hamiltonian
@@ -68,7 +69,7 @@ def test_si64_variants_match_the_reference(si_pseudo):
     H = Hamiltonian(s, veff.cpu().numpy(), precision="complex64")
     eng = H.engine
     variants = _available(eng, "complex64")
-    assert variants == [0, 1, 2]
+    assert variants == [0, 1, 2, 3]
     for v in variants:
         eng.set_stage_b_variant("complex64", v)
         for ik, nbk in ((0, 2), (1, 1)):
