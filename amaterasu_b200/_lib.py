@@ -53,6 +53,9 @@ SIGNATURES = {
     "ama_version": (ct.c_int, []),
     "ama_engine_create": (ct.c_int, [ct.POINTER(AmaSystemDesc), ct.POINTER(_P)]),
     "ama_engine_destroy": (ct.c_int, [_P]),
+    "ama_grid_gradient": (ct.c_int, [_P, _P, _P, ct.c_double, _P, _P]),
+    "ama_grid_divergence": (ct.c_int, [_P, _P, _P, ct.c_double, ct.c_double, _P, _P]),
+    "ama_xc_gga": (ct.c_int, [_P, _I32, _I32, _P, _P, _P, _P, _P]),
     "ama_engine_option": (ct.c_int, [_P, _I32, _I32]),
     "ama_tc_status": (ct.c_int, [_P, ct.POINTER(ct.c_int32)]),
     "ama_set_potential": (ct.c_int, [_P, _P, _I32, _P]),

@@ -3,8 +3,9 @@
 The engine compiles several variants of the x-transform stage ("stage B": shared-memory
 slabs; register-resident x columns for short x lines; register-resident with the spheres'
 x-plane set fixed at compile time, for the benchmark grid; register-resident with two
-threads per column, for even x lengths up to 108) and two paths for the complex64
-nonlocal products (tcgen05 split-TF32 GEMMs or SIMT GEMMs). Which is fastest depends on the
+threads per column, for even x lengths up to 108), two variants of the stages around it
+(y transforms in shared memory or in registers with four lanes per column) and two paths
+for the complex64 nonlocal products (tcgen05 split-TF32 GEMMs or SIMT GEMMs). Which is fastest depends on the
 grid, the band count and the number of k-points of a call. ``autotune_hpsi`` times every
 available combination on the caller's Hamiltonian and block shape (CUDA events on the
 current stream after one warm-up call each), leaves the engine set to the fastest and
@@ -30,11 +31,25 @@ def _variants(eng, prec_code):
     return out
 
 
+def _ac_variants(eng, prec_code):
+    """complex64 stage A/C variants the engine has (complex128 has only the first)."""
+    if prec_code != 0:
+        return [0]
+    out = []
+    for v in (0, 1):
+        try:
+            eng.set_stage_ac_variant(v)
+            out.append(v)
+        except NotImplementedError:
+            pass
+    return out
+
+
 def autotune_hpsi(H, nbands: int, *, k_first: int = 0, k_count: int | None = None, reps: int = 3,
                   force: bool = False) -> dict:
-    """Time the stage B variants x nonlocal paths for ``H.apply_all`` on blocks of ``nbands``
-    bands at k-points k_first .. k_first + k_count - 1, select the fastest on H's engine and
-    return ``{"stage_b": v, "nonlocal_tc": bool, "ms": {(v, tc): ms}}``."""
+    """Time the stage B variants x stage A/C variants x nonlocal paths for ``H.apply_all`` on
+    blocks of ``nbands`` bands at k-points k_first .. k_first + k_count - 1, select the fastest
+    on H's engine and return ``{"stage_b": v, "stage_ac": a, "nonlocal_tc": bool, "ms": {...}}``."""
     eng = H.engine
     prec = precision_code(H.precision)
     k_count = eng.nk - k_first if k_count is None else k_count
@@ -45,6 +60,8 @@ def autotune_hpsi(H, nbands: int, *, k_first: int = 0, k_count: int | None = Non
     if key in cache and not force:
         choice = cache[key]
         eng.set_stage_b_variant(prec, choice["stage_b"])
+        if prec == 0:
+            eng.set_stage_ac_variant(choice["stage_ac"])
         eng.set_tensor_core_nonlocal(choice["nonlocal_tc"])
         return choice
     n = int(eng.pw_off[k_first + k_count] - eng.pw_off[k_first]) * nbands
@@ -56,20 +73,25 @@ def autotune_hpsi(H, nbands: int, *, k_first: int = 0, k_count: int | None = Non
     stream = torch.cuda.current_stream(eng.device)
     for v in _variants(eng, prec):
         eng.set_stage_b_variant(prec, v)
-        for tc in paths:
-            eng.set_tensor_core_nonlocal(tc)
-            H.apply_all(psi, nbands, k_first=k_first, k_count=k_count, out=out)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            for _ in range(reps):
+        for a in _ac_variants(eng, prec):
+            if prec == 0:
+                eng.set_stage_ac_variant(a)
+            for tc in paths:
+                eng.set_tensor_core_nonlocal(tc)
                 H.apply_all(psi, nbands, k_first=k_first, k_count=k_count, out=out)
-            e1.record(stream)
-            torch.cuda.synchronize(eng.device)
-            times[(v, tc)] = e0.elapsed_time(e1) / reps
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                for _ in range(reps):
+                    H.apply_all(psi, nbands, k_first=k_first, k_count=k_count, out=out)
+                e1.record(stream)
+                torch.cuda.synchronize(eng.device)
+                times[(v, a, tc)] = e0.elapsed_time(e1) / reps
     best = min(times, key=times.get)
     eng.set_stage_b_variant(prec, best[0])
-    eng.set_tensor_core_nonlocal(best[1])
-    choice = {"stage_b": best[0], "nonlocal_tc": best[1],
-              "ms": {f"stage_b={v},nonlocal_tc={int(tc)}": ms for (v, tc), ms in times.items()}}
+    if prec == 0:
+        eng.set_stage_ac_variant(best[1])
+    eng.set_tensor_core_nonlocal(best[2])
+    choice = {"stage_b": best[0], "stage_ac": best[1], "nonlocal_tc": best[2],
+              "ms": {f"stage_b={v},stage_ac={a},nonlocal_tc={int(tc)}": ms for (v, a, tc), ms in times.items()}}
     cache[key] = choice
     return choice

@@ -234,10 +234,8 @@ class BatchedDavidson:
             self.trace.append((it, nn, m, float(norms.max())))
             if nn == 0:
                 break
-            rows = np.full((self.nk, nb), -1, dtype=np.int32)
-            for k in range(self.nk):
-                idx = np.nonzero(active[k])[0]
-                rows[k, idx] = np.arange(len(idx), dtype=np.int32)
+            # row of each active band in its k-point's correction block (-1: inactive)
+            rows = np.where(active, np.cumsum(active, axis=1) - 1, -1).astype(np.int32)
             rows_t = torch.from_numpy(rows).to(self.dev)
             C = self._blocks(nn)
             call("ama_kbatch_residual", self.prec, self.nk, nb, ptr(self.npw), ptr(self.pw_off), ptr(X), ptr(HX),

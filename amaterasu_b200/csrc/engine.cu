@@ -103,6 +103,7 @@ struct DynDims {
   template <class V> __device__ static __forceinline__ int a3(const V& v) { return v.A3; }
 };
 template <int N1, int A1, int N2, int A2, int N3, int A3> struct FixDims {
+  static constexpr int n3c() { return N3; }
   // stage B may split each (x, z) slab into z parts (less shared memory per CTA); measured
   // slower at the benchmark grids, so one part
   static constexpr int zsplit = 1;
@@ -150,6 +151,78 @@ __device__ __forceinline__ void async_copy(C* dst, const C* src, int n) {
 
 __device__ __forceinline__ void async_copy_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
+// Zero the (n2, n3) slot plane, load the list of its rows that hold sphere points, and
+// scatter the band's coefficients into it (four entries per thread in flight: the psi load
+// depends on the entry load). NT threads; ends with a barrier. Returns the row count.
+template <int NT, typename C>
+__device__ __forceinline__ int plane_scatter(const HpsiView& v, int plane, int k, int slot,
+                                             const C* __restrict__ src, C* pl, int* rows) {
+  for (int i = threadIdx.x; i < plane; i += NT) pl[i] = mk<C>(0, 0);
+  const int rs = v.row_start[k * (v.nslots + 1) + slot];
+  const int nrows = v.row_start[k * (v.nslots + 1) + slot + 1] - rs;
+  for (int i = threadIdx.x; i < nrows; i += NT) rows[i] = v.rows[rs + i];
+  __syncthreads();
+  const int es = v.entry_start[k * (v.nslots + 1) + slot];
+  const int ee = v.entry_start[k * (v.nslots + 1) + slot + 1];
+  int t = es + threadIdx.x;
+  for (; t + 3 * NT < ee; t += 4 * NT) {
+    int2 en[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) en[u] = v.entries[t + u * NT];
+    C val[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) val[u] = src[en[u].x];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) pl[en[u].y] = val[u];
+  }
+  for (; t < ee; t += NT) {
+    const int2 en = v.entries[t];
+    pl[en.y] = src[en.x];
+  }
+  __syncthreads();
+  return nrows;
+}
+
+// Gather the band's sphere points out of the transformed plane and add the kinetic term:
+// hpsi = plane value + T_G psi (four entries per thread in flight). NT threads.
+template <int NT, typename T>
+__device__ __forceinline__ void plane_gather(const HpsiView& v, int k, int slot, const cx_t<T>* pl,
+                                             const T* __restrict__ kk, const cx_t<T>* __restrict__ psi,
+                                             cx_t<T>* __restrict__ hpsi, int64_t boff) {
+  using C = cx_t<T>;
+  const int es = v.entry_start[k * (v.nslots + 1) + slot];
+  const int ee = v.entry_start[k * (v.nslots + 1) + slot + 1];
+  int t = es + threadIdx.x;
+  for (; t + 3 * NT < ee; t += 4 * NT) {
+    int2 en[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) en[u] = v.entries[t + u * NT];
+    C p[4];
+    T tg[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      p[u] = psi[boff + en[u].x];
+      tg[u] = kk[en[u].x];
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      C r = pl[en[u].y];
+      r.x += tg[u] * p[u].x;
+      r.y += tg[u] * p[u].y;
+      hpsi[boff + en[u].x] = r;
+    }
+  }
+  for (; t < ee; t += NT) {
+    const int2 en = v.entries[t];
+    const C p = psi[boff + en.x];
+    C r = pl[en.y];
+    const T tg = kk[en.x];
+    r.x += tg * p.x;
+    r.y += tg * p.y;
+    hpsi[boff + en.x] = r;
+  }
+}
+
 template <typename T, class D>
 __global__ void __launch_bounds__(kFftThreads)
 stage_a_kernel(HpsiView v, const cx_t<T>* __restrict__ tw_y, const cx_t<T>* __restrict__ tw_z,
@@ -171,30 +244,7 @@ stage_a_kernel(HpsiView v, const cx_t<T>* __restrict__ tw_y, const cx_t<T>* __re
 
   load_tw(sty, tw_y, n2);
   load_tw(stz, tw_z, n3);
-  for (int i = threadIdx.x; i < plane; i += kFftThreads) pl[i] = mk<C>(0, 0);
-  const int rs = v.row_start[k * (v.nslots + 1) + slot];
-  const int nrows = v.row_start[k * (v.nslots + 1) + slot + 1] - rs;
-  for (int i = threadIdx.x; i < nrows; i += kFftThreads) rows[i] = v.rows[rs + i];
-  __syncthreads();
-  const int es = v.entry_start[k * (v.nslots + 1) + slot];
-  const int ee = v.entry_start[k * (v.nslots + 1) + slot + 1];
-  // scatter, four entries per thread in flight (the psi load depends on the entry load)
-  int t = es + threadIdx.x;
-  for (; t + 3 * kFftThreads < ee; t += 4 * kFftThreads) {
-    int2 en[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) en[u] = v.entries[t + u * kFftThreads];
-    C val[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) val[u] = src[en[u].x];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) pl[en[u].y] = val[u];
-  }
-  for (; t < ee; t += kFftThreads) {
-    const int2 en = v.entries[t];
-    pl[en.y] = src[en.x];
-  }
-  __syncthreads();
+  const int nrows = plane_scatter<kFftThreads>(v, plane, k, slot, src, pl, rows);
   dft_rows<+1>(pl, n3, A3, B3, n3, rows, nrows, stz);
   dft_cols<+1>(pl, n2, A2, B2, n3, sty);
   C* dst = work + (int64_t)gb * v.band_elems + (int64_t)slot * plane;
@@ -507,39 +557,175 @@ stage_c_kernel(HpsiView v, const cx_t<T>* __restrict__ tw_y, const cx_t<T>* __re
   __syncthreads();
   dft_cols<-1>(pl, n2, A2, B2, n3, sty);
   dft_rows<-1>(pl, n3, A3, B3, n3, rows, nrows, stz);
-  const int es = v.entry_start[k * (v.nslots + 1) + slot];
-  const int ee = v.entry_start[k * (v.nslots + 1) + slot + 1];
-  const T* kk = kin + v.pw_off[k];
-  // gather + T psi, four entries per thread in flight
-  int t = es + threadIdx.x;
-  for (; t + 3 * kFftThreads < ee; t += 4 * kFftThreads) {
-    int2 en[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) en[u] = v.entries[t + u * kFftThreads];
-    C p[4];
-    T tg[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      p[u] = psi[boff + en[u].x];
-      tg[u] = kk[en[u].x];
-    }
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      C r = pl[en[u].y];
-      r.x += tg[u] * p[u].x;
-      r.y += tg[u] * p[u].y;
-      hpsi[boff + en[u].x] = r;
+  plane_gather<kFftThreads, T>(v, k, slot, pl, kin + v.pw_off[k], psi, hpsi, boff);
+}
+
+// ------------------------------------------- y transforms in registers, four lanes per column
+// Stages A and C of complex64 H.psi with the y transform of each (slot, band) plane done in
+// registers instead of two shared-memory passes over the whole plane: four adjacent lanes
+// share a z column, lane h holding the M = n2 / 4 values of y index 4 m + h. Backward, each
+// lane transforms its values with a length-M register DFT (Y_h[k] = sum_m u[4m+h] w_M^{mk})
+// and the lanes combine them by
+//   X[k + M j] = sum_h (w^{hk} Y_h[k]) i^{hj}          (w = e^{2 pi i / n2})
+// as a 4-point DFT across the lanes in two butterfly steps (shuffles with lane distance 2,
+// then 1), after which lane h = h0 + 2 h1 holds X[k + M (h1 + 2 h0)]. The forward transform
+// is the adjoint of the same steps in reverse order, ending with length-M register DFTs
+// whose outputs are y = 4 m + h. Stage A writes its registers straight to the slot plane in
+// HBM (the engine's permuted y order), stage C loads them straight from it, so besides
+// the y passes the plane copy through shared memory is gone too. The z transforms (rows
+// with sphere points only) stay in shared memory.
+template <int N3>
+constexpr int quad_threads() { return (4 * N3 + 31) / 32 * 32; }
+
+template <int N, int M, int AH>
+__host__ __device__ constexpr int quad_index(int p) { return half_index<M, AH>(p); }
+
+// a * w^{S h K} for the lane's h in 0..3 (w = e^{2 pi i / N}), twiddles as immediates
+template <int N, int S, int K>
+__device__ __forceinline__ float2 quad_twiddle(float2 a, int h) {
+  if constexpr (K == 0) {
+    return a;
+  } else {
+    constexpr float c1 = (float)LineTwiddles<N>::cos[K % N], s1 = (float)(S * LineTwiddles<N>::sin[K % N]);
+    constexpr float c2 = (float)LineTwiddles<N>::cos[2 * K % N], s2 = (float)(S * LineTwiddles<N>::sin[2 * K % N]);
+    constexpr float c3 = (float)LineTwiddles<N>::cos[3 * K % N], s3 = (float)(S * LineTwiddles<N>::sin[3 * K % N]);
+    const float c = h == 0 ? 1.f : (h == 1 ? c1 : (h == 2 ? c2 : c3));
+    const float sn = h == 0 ? 0.f : (h == 1 ? s1 : (h == 2 ? s2 : s3));
+    return make_float2(a.x * c - a.y * sn, a.x * sn + a.y * c);
+  }
+}
+
+__device__ __forceinline__ float2 shfl_xor_c(float2 a, int d) {
+  return make_float2(__shfl_xor_sync(0xffffffffu, a.x, d), __shfl_xor_sync(0xffffffffu, a.y, d));
+}
+
+// backward: r[p] = Y_h[k] (k = quad_index(p)) -> X[k + M (h1 + 2 h0)]
+template <int N, int M, int AH>
+__device__ __forceinline__ void quad_combine_backward(float2 (&r)[M], int h) {
+  const int h0 = h & 1, h1 = h >> 1;
+  static_for<M>([&](auto pp) {
+    constexpr int p = decltype(pp)::value;
+    constexpr int k = quad_index<N, M, AH>(p);
+    const float2 t = quad_twiddle<N, +1, k>(r[p], h);
+    const float2 o = shfl_xor_c(t, 2);
+    const float2 u = h1 ? csub(o, t) : cadd(t, o);  // U_{h0}(j parity h1)
+    const float2 q = shfl_xor_c(u, 1);
+    const float2 u0 = h0 ? q : u, u1 = h0 ? u : q;
+    const float2 v = h1 ? make_float2(-u1.y, u1.x) : u1;  // i^{h1} U_1
+    r[p] = h0 ? csub(u0, v) : cadd(u0, v);
+  });
+}
+
+// forward, the adjoint: r[p] = X[k + M (h1 + 2 h0)] -> Z_h[k] = w^{-hk} sum_j X[k + M j] (-i)^{hj}
+template <int N, int M, int AH>
+__device__ __forceinline__ void quad_combine_forward(float2 (&r)[M], int h) {
+  const int h0 = h & 1, h1 = h >> 1;
+  static_for<M>([&](auto pp) {
+    constexpr int p = decltype(pp)::value;
+    constexpr int k = quad_index<N, M, AH>(p);
+    const float2 a = r[p];
+    const float2 q = shfl_xor_c(a, 1);
+    const float2 d = csub(q, a);                              // (lane h0=0) - (lane h0=1), seen from h0=1
+    const float2 u1 = h1 ? make_float2(d.y, -d.x) : d;        // conj(i^{h1}) (a - b)
+    const float2 u = h0 ? u1 : cadd(a, q);
+    const float2 o = shfl_xor_c(u, 2);
+    const float2 t = h1 ? csub(o, u) : cadd(u, o);
+    r[p] = quad_twiddle<N, -1, k>(t, h);
+  });
+}
+
+template <int NY, int AQ, class D>
+__global__ void __launch_bounds__(quad_threads<D::n3c()>())
+stage_a_quad_kernel(HpsiView v, const float2* __restrict__ tw_y, const float2* __restrict__ tw_z,
+                    const float2* __restrict__ psi, float2* __restrict__ work) {
+  using C = float2;
+  constexpr int NT = quad_threads<D::n3c()>();
+  constexpr int M = NY / 4;
+  AMA_DIMS(D, v)
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* pl = reinterpret_cast<C*>(smem_raw);
+  C* stz = pl + plane + n2;  // the shared layout of stage A (no y twiddles needed)
+  int* rows = reinterpret_cast<int*>(stz + n3);
+
+  const int slot = blockIdx.x;
+  const int gb = blockIdx.y;
+  const int kl = gb / v.nbands, band = gb - kl * v.nbands;
+  const int k = v.k_first + kl;
+  const int npw = v.npw[k];
+  const C* src = psi + (v.pw_off[k] - v.pw_off[v.k_first]) * v.nbands + (int64_t)band * npw;
+  for (int i = threadIdx.x; i < n3; i += NT) stz[i] = tw_z[i];
+  const int nrows = plane_scatter<NT>(v, plane, k, slot, src, pl, rows);
+  dft_rows<+1, true, NT>(pl, n3, A3, B3, n3, rows, nrows, stz);
+  // y columns: lanes 4c .. 4c+3 take column c; lanes past the last column shuffle along
+  const int col_raw = threadIdx.x >> 2, h = threadIdx.x & 3;
+  if ((int)(threadIdx.x & ~31u) >= 4 * n3) return;  // the whole warp is past the last column
+  const bool live = col_raw < n3;
+  const int col = live ? col_raw : 0;
+  float2 r[M];
+  static_for<M>([&](auto mm) {
+    constexpr int m = decltype(mm)::value;
+    r[m] = pl[(4 * m + h) * n3 + col];
+  });
+  dft_line_reg<M, AQ, +1, true>(r, tw_y);
+  quad_combine_backward<NY, M, AQ>(r, h);
+  if (!live) return;
+  C* dst = work + (int64_t)gb * v.band_elems + (int64_t)slot * plane + col;
+  const int j = (h >> 1) + 2 * (h & 1);
+  static_for<M>([&](auto pp) {
+    constexpr int p = decltype(pp)::value;
+    const int i = quad_index<NY, M, AQ>(p) + M * j;  // natural y index held in r[p]
+    dst[(int64_t)((i % A2) * B2 + i / A2) * n3] = r[p];
+  });
+}
+
+template <int NY, int AQ, class D>
+__global__ void __launch_bounds__(quad_threads<D::n3c()>())
+stage_c_quad_kernel(HpsiView v, const float2* __restrict__ tw_y, const float2* __restrict__ tw_z,
+                    const float* __restrict__ kin, const float2* __restrict__ psi,
+                    const float2* __restrict__ work, float2* __restrict__ hpsi) {
+  using C = float2;
+  constexpr int NT = quad_threads<D::n3c()>();
+  constexpr int M = NY / 4;
+  AMA_DIMS(D, v)
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* pl = reinterpret_cast<C*>(smem_raw);
+  C* stz = pl + plane + n2;
+  int* rows = reinterpret_cast<int*>(stz + n3);
+
+  const int slot = blockIdx.x;
+  const int gb = blockIdx.y;
+  const int kl = gb / v.nbands, band = gb - kl * v.nbands;
+  const int k = v.k_first + kl;
+  const int npw = v.npw[k];
+  const int64_t boff = (v.pw_off[k] - v.pw_off[v.k_first]) * v.nbands + (int64_t)band * npw;
+  for (int i = threadIdx.x; i < n3; i += NT) stz[i] = tw_z[i];
+  const int rs = v.row_start[k * (v.nslots + 1) + slot];
+  const int nrows = v.row_start[k * (v.nslots + 1) + slot + 1] - rs;
+  for (int i = threadIdx.x; i < nrows; i += NT) rows[i] = v.rows[rs + i];
+  const int col_raw = threadIdx.x >> 2, h = threadIdx.x & 3;
+  if ((int)(threadIdx.x & ~31u) < 4 * n3) {  // warps with at least one live column
+    const bool live = col_raw < n3;
+    const int col = live ? col_raw : 0;
+    const C* srcw = work + (int64_t)gb * v.band_elems + (int64_t)slot * plane + col;
+    const int j = (h >> 1) + 2 * (h & 1);
+    float2 r[M];
+    static_for<M>([&](auto pp) {
+      constexpr int p = decltype(pp)::value;
+      const int i = quad_index<NY, M, AQ>(p) + M * j;
+      r[p] = __ldg(srcw + (int64_t)((i % A2) * B2 + i / A2) * n3);
+    });
+    quad_combine_forward<NY, M, AQ>(r, h);
+    dft_line_reg<M, AQ, -1, false>(r, tw_y);
+    if (live) {
+      static_for<M>([&](auto mm) {
+        constexpr int m = decltype(mm)::value;
+        pl[(4 * m + h) * n3 + col] = r[m];
+      });
     }
   }
-  for (; t < ee; t += kFftThreads) {
-    const int2 en = v.entries[t];
-    const C p = psi[boff + en.x];
-    C r = pl[en.y];
-    const T tg = kk[en.x];
-    r.x += tg * p.x;
-    r.y += tg * p.y;
-    hpsi[boff + en.x] = r;
-  }
+  __syncthreads();
+  dft_rows<-1, false, NT>(pl, n3, A3, B3, n3, rows, nrows, stz);
+  plane_gather<NT, float>(v, k, slot, pl, kin + v.pw_off[k], psi, hpsi, boff);
 }
 
 // density: stage A output -> backward x, then weighted |u|^2 into a permuted FP64 grid.
@@ -570,10 +756,14 @@ density_b_kernel(HpsiView v, const cx_t<T>* __restrict__ tw_xb, const cx_t<T>* _
 // The stage B variants compiled for a grid: [0] shared-memory slab, [1] register-resident
 // x columns, [2] register-resident with the compile-time slot set, [3] register-resident
 // with two threads per column (null when absent).
+// The stage A/C pairs: [0] shared-memory y passes, [1] y transforms in registers with four
+// lanes per column (null when absent), with their threads per CTA.
 struct StageInfo {
   int zsplit;
   bool regb;
   const void* b_variant[4];
+  const void* ac_variant[2][2] = {};
+  int ac_threads[2] = {kFftThreads, kFftThreads};
 };
 
 template <typename T, class D>
@@ -582,17 +772,32 @@ StageInfo fill_stage_table(const void** fn) {
   fn[1] = (const void*)stage_b_kernel<T, D>;
   fn[2] = (const void*)stage_c_kernel<T, D>;
   fn[3] = (const void*)density_b_kernel<T, D>;
-  return {D::zsplit, false, {fn[1], nullptr, nullptr}};
+  StageInfo info{D::zsplit, false, {fn[1], nullptr, nullptr}};
+  info.ac_variant[0][0] = fn[0];
+  info.ac_variant[0][1] = fn[2];
+  return info;
 }
 
-// complex64 on a compile-time grid with short x columns: register-resident stage B
-// (register-resident y columns for stages A and C were measured slower than the
-// shared-memory passes at 84^3 and are not used)
+// the four-lanes-per-column stages A and C, when n2 = 4 M with a nontrivial split of M and
+// both y lengths have immediate twiddles
+template <int N2, class D>
+void add_quad_variant(StageInfo& info) {
+  if constexpr (N2 % 4 == 0 && N2 >= 80) {  // short y lines stay with the shared-memory passes
+    constexpr int M = N2 / 4;
+    constexpr int AQ = M % 3 == 0 && M > 3 ? 3 : (M % 2 == 0 && M > 2 ? 2 : 0);
+    if constexpr (AQ > 0 && LineTwiddles<M>::kHave && LineTwiddles<N2>::kHave) {
+      info.ac_variant[1][0] = (const void*)stage_a_quad_kernel<N2, AQ, D>;
+      info.ac_variant[1][1] = (const void*)stage_c_quad_kernel<N2, AQ, D>;
+      info.ac_threads[1] = quad_threads<D::n3c()>();
+    }
+  }
+}
+
 // the two-lanes-per-column stage B, when n1 is even and both line lengths have immediate
 // twiddles (the half-length DFT cannot take its twiddles from the n1 table)
 template <int N1, class D>
 void add_pair_variant(StageInfo& info) {
-  if constexpr (N1 % 2 == 0) {
+  if constexpr (N1 % 2 == 0 && N1 >= 40) {  // shorter lines fit one thread's registers
     constexpr int M = N1 / 2;
     if constexpr (LineTwiddles<M>::kHave && LineTwiddles<N1>::kHave) {
       constexpr int AH = M % 6 == 0 && M / 6 > 1 ? 6 : (M % 3 == 0 ? 3 : (M % 2 == 0 ? 2 : M));
@@ -601,6 +806,9 @@ void add_pair_variant(StageInfo& info) {
   }
 }
 
+// complex64 on a compile-time grid with short x columns: register-resident stage B
+// (register-resident y columns for stages A and C were measured slower than the
+// shared-memory passes at 84^3 and are not used)
 template <int N1, int A1, int N2, int A2, int N3, class D>
 StageInfo fill_stage_table_reg(const void** fn, int hp, int hn) {
   StageInfo info = fill_stage_table<float, D>(fn);
@@ -608,6 +816,7 @@ StageInfo fill_stage_table_reg(const void** fn, int hp, int hn) {
   info.regb = true;
   info.b_variant[1] = fn[1];
   add_pair_variant<N1, D>(info);
+  add_quad_variant<N2, D>(info);
   if constexpr (N1 == 84) {  // the Si64 benchmark grid: sparse-x variants for its slot sets
 #define AMA_SPARSE(P, Q) \
     if (hp == P && hn == Q) fn[1] = info.b_variant[2] = (const void*)stage_b_sparse_kernel<84, 12, P, Q, D>;
@@ -630,6 +839,7 @@ StageInfo select_stage_table(const AxisPlan* ax, const void** fn, int hp, int hn
     } else if constexpr (std::is_same<T, float>::value) { /* longer x lines: only two lanes */   \
       StageInfo info = fill_stage_table<T, D>(fn);                                               \
       add_pair_variant<N1, D>(info);                                                             \
+      add_quad_variant<N2, D>(info);                                                             \
       return info;                                                                               \
     } else {                                                                                     \
       return fill_stage_table<T, D>(fn);                                                         \
@@ -655,6 +865,7 @@ using StageCFn = void (*)(HpsiView, const cx_t<T>*, const cx_t<T>*, const T*, co
                           const cx_t<T>*, cx_t<T>*);
 template <typename T>
 using DensFn = void (*)(HpsiView, const cx_t<T>*, const cx_t<T>*, const double*, double*);
+
 
 template <typename T>
 __global__ void permute_potential_kernel(const double* __restrict__ v, T* __restrict__ out,
@@ -759,6 +970,17 @@ int set_smem_limits(const AmaEngine* e) {
   const_cast<AmaEngine*>(e)->regb[p] = info.regb;
   const_cast<AmaEngine*>(e)->bthreads[p] = 1;
   for (int i = 0; i < 4; ++i) const_cast<AmaEngine*>(e)->b_variant[p][i] = info.b_variant[i];
+  for (int i = 0; i < 2; ++i) {
+    const_cast<AmaEngine*>(e)->ac_variant[p][i][0] = info.ac_variant[i][0];
+    const_cast<AmaEngine*>(e)->ac_variant[p][i][1] = info.ac_variant[i][1];
+    const_cast<AmaEngine*>(e)->ac_threads_of[p][i] = info.ac_threads[i];
+    if (info.ac_variant[i][0]) {
+      AMA_CUDA_TRY(cudaFuncSetAttribute(info.ac_variant[i][0], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
+      AMA_CUDA_TRY(cudaFuncSetAttribute(info.ac_variant[i][1], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
+    }
+  }
+  const_cast<AmaEngine*>(e)->ac_threads[p] = kFftThreads;
+
   AMA_CUDA_TRY(cudaFuncSetAttribute(fn[0], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
   AMA_CUDA_TRY(cudaFuncSetAttribute(fn[2], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
   AMA_CUDA_TRY(cudaFuncSetAttribute(info.b_variant[0], cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -786,7 +1008,7 @@ int run_fft_stages_a(AmaEngine* e, const HpsiView& v, int nb_total, const void* 
   using C = cx_t<T>;
   const int p = std::is_same<T, float>::value ? AMA_C64 : AMA_C128;
   dim3 ga(e->nslots, nb_total);
-  ((StageAFn<T>)e->stage_fn[p][0])<<<ga, kFftThreads, plane_smem<T>(e), s>>>(
+  ((StageAFn<T>)e->stage_fn[p][0])<<<ga, e->ac_threads[p], plane_smem<T>(e), s>>>(
       v, (const C*)e->d.tw[p][1][0], (const C*)e->d.tw[p][2][0], (const C*)psi, (C*)e->work[p]);
   AMA_CHECK_LAUNCH();
   return AMA_OK;
@@ -824,7 +1046,7 @@ int hpsi_impl(AmaEngine* e, int k_first, int k_count, int nbands, int spin, cons
   }
   AMA_CHECK_LAUNCH();
   dim3 gc(e->nslots, nb_total);
-  ((StageCFn<T>)e->stage_fn[p][2])<<<gc, kFftThreads, plane_smem<T>(e), s>>>(
+  ((StageCFn<T>)e->stage_fn[p][2])<<<gc, e->ac_threads[p], plane_smem<T>(e), s>>>(
       v, (const C*)e->d.tw[p][1][1], (const C*)e->d.tw[p][2][1], kin, (const C*)psi,
       (const C*)e->work[p], (C*)hpsi);
   AMA_CHECK_LAUNCH();
@@ -1337,6 +1559,129 @@ __global__ void __launch_bounds__(kFftThreads) grid_g2f_kernel(GridView g, const
 }  // namespace
 
 namespace {
+// i G_a / N (times a caller scale) at the forward transform's storage position (p1, p2, p3):
+// G = sum_i m_i b_i with m the signed frequency of each axis, zero at the Nyquist frequency
+// of an even axis (the spectral derivative of a real field stays real).
+struct Recip {
+  double b[3][3];  // rows: reciprocal lattice vectors b_1, b_2, b_3 (Cartesian, 1/Bohr)
+};
+
+__device__ __forceinline__ int signed_freq(int p, int n, int A, int B) {
+  const int f = p / B + A * (p % B);  // natural frequency index held at storage position p
+  if (2 * f == n) return 0;           // Nyquist of an even axis
+  return 2 * f > n ? f - n : f;
+}
+
+// G2 of the spectral gradient: slab y of the G1 output, forward x, times i G_a scale / N,
+// backward x, into work_out + a N (a = blockIdx.y).
+__global__ void __launch_bounds__(kFftThreads) grid_g2_grad_kernel(GridView g, const double2* tw_f, const double2* tw_b,
+                                    Recip rc, double scale, const double2* __restrict__ work_in,
+                                    double2* __restrict__ work_out) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* slab = reinterpret_cast<double2*>(smem_raw);
+  double2* twf = slab + (int64_t)g.n1 * g.n3;
+  double2* twb = twf + g.n1;
+  const int p2 = blockIdx.x, axis = blockIdx.y;
+  load_twiddles(twf, tw_f, g.n1);
+  load_twiddles(twb, tw_b, g.n1);
+  const double2* wb = work_in + (int64_t)p2 * g.n3;
+  const int total = g.n1 * g.n3;
+  for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    const int x = e / g.n3, z = e % g.n3;
+    slab[e] = wb[(int64_t)x * g.plane_elems + z];
+  }
+  __syncthreads();
+  dft_cols<-1, true>(slab, g.n1, g.A1, g.B1, g.n3, twf);
+  const int m2 = signed_freq(p2, g.n2, g.A2, g.B2);
+  for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    const int p1 = e / g.n3, p3 = e % g.n3;
+    const int m1 = signed_freq(p1, g.n1, g.A1, g.B1), m3 = signed_freq(p3, g.n3, g.A3, g.B3);
+    const double ga = (m1 * rc.b[0][axis] + m2 * rc.b[1][axis] + m3 * rc.b[2][axis]) * scale;
+    const double2 c = slab[e];
+    slab[e] = make_double2(-ga * c.y, ga * c.x);  // i G_a c
+  }
+  __syncthreads();
+  dft_cols<+1, false>(slab, g.n1, g.A1, g.B1, g.n3, twb);
+  double2* ob = work_out + (int64_t)axis * g.n1 * g.plane_elems + (int64_t)p2 * g.n3;
+  for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    const int x = e / g.n3, z = e % g.n3;
+    ob[(int64_t)x * g.plane_elems + z] = slab[e];
+  }
+}
+
+// G2 of the spectral divergence: for each component a, slab y of its G1 output (work + a N),
+// forward x, times i G_a scale / N, summed over a (the running sum kept in component 0's
+// slab, which only this CTA touches), then backward x into component 0.
+__global__ void __launch_bounds__(kFftThreads) grid_g2_div_kernel(GridView g, const double2* tw_f, const double2* tw_b,
+                                   Recip rc, double scale, double2* __restrict__ work) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* slab = reinterpret_cast<double2*>(smem_raw);
+  double2* twf = slab + (int64_t)g.n1 * g.n3;
+  double2* twb = twf + g.n1;
+  const int p2 = blockIdx.x;
+  load_twiddles(twf, tw_f, g.n1);
+  load_twiddles(twb, tw_b, g.n1);
+  const int total = g.n1 * g.n3;
+  const int64_t field = (int64_t)g.n1 * g.plane_elems;
+  double2* acc = work + (int64_t)p2 * g.n3;
+  const int m2 = signed_freq(p2, g.n2, g.A2, g.B2);
+  for (int axis = 0; axis < 3; ++axis) {
+    const double2* wb = work + axis * field + (int64_t)p2 * g.n3;
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+      const int x = e / g.n3, z = e % g.n3;
+      slab[e] = wb[(int64_t)x * g.plane_elems + z];
+    }
+    __syncthreads();
+    dft_cols<-1, true>(slab, g.n1, g.A1, g.B1, g.n3, twf);
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+      const int p1 = e / g.n3, p3 = e % g.n3;
+      const int m1 = signed_freq(p1, g.n1, g.A1, g.B1), m3 = signed_freq(p3, g.n3, g.A3, g.B3);
+      const double ga = (m1 * rc.b[0][axis] + m2 * rc.b[1][axis] + m3 * rc.b[2][axis]) * scale;
+      const double2 c = slab[e];
+      double2 t = make_double2(-ga * c.y, ga * c.x);
+      const int64_t gi = (int64_t)p1 * g.plane_elems + p3;  // this thread's own element
+      if (axis > 0) {
+        const double2 prev = acc[gi];
+        t.x += prev.x;
+        t.y += prev.y;
+      }
+      if (axis < 2) acc[gi] = t;
+      else slab[e] = t;
+    }
+    __syncthreads();
+  }
+  dft_cols<+1, false>(slab, g.n1, g.A1, g.B1, g.n3, twb);
+  for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    const int x = e / g.n3, z = e % g.n3;
+    acc[(int64_t)x * g.plane_elems + z] = slab[e];
+  }
+}
+
+// G3 that adds: out = beta out + alpha Re(backward y, z of the plane).
+__global__ void __launch_bounds__(kFftThreads) grid_g3_axpy_kernel(GridView g, const double2* tw_y, const double2* tw_z,
+                                    const double2* __restrict__ work, double alpha, double beta,
+                                    double* __restrict__ out) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* plane = reinterpret_cast<double2*>(smem_raw);
+  double2* sty = plane + g.plane_elems;
+  double2* stz = sty + g.n2;
+  int* rows = reinterpret_cast<int*>(stz + g.n3);
+  const int x = blockIdx.x;
+  load_twiddles(sty, tw_y, g.n2);
+  load_twiddles(stz, tw_z, g.n3);
+  for (int i = threadIdx.x; i < g.n2; i += blockDim.x) rows[i] = i;
+  const double2* src = work + (int64_t)x * g.plane_elems;
+  for (int64_t i = threadIdx.x; i < g.plane_elems; i += blockDim.x) plane[i] = src[i];
+  __syncthreads();
+  dft_cols<+1, false>(plane, g.n2, g.A2, g.B2, g.n3, sty);
+  dft_rows<+1, false>(plane, g.n3, g.A3, g.B3, g.n3, rows, g.n2, stz);
+  double* dst = out + (int64_t)x * g.plane_elems;
+  for (int64_t i = threadIdx.x; i < g.plane_elems; i += blockDim.x)
+    dst[i] = (beta == 0.0 ? 0.0 : beta * dst[i]) + alpha * plane[i].x;
+}
+}  // namespace
+
+namespace {
 void free_grid_filters(AmaEngine* e) {
   for (double*& p : e->grid_filt) {
     if (p) cudaFree(p);
@@ -1347,8 +1692,8 @@ void free_grid_filters(AmaEngine* e) {
   e->grid_work_bytes = 0;
 }
 
-int ensure_grid_work(AmaEngine* e) {
-  const size_t need = (size_t)e->N * sizeof(double2);
+int ensure_grid_work(AmaEngine* e, int fields = 1) {
+  const size_t need = (size_t)fields * e->N * sizeof(double2);
   if (e->grid_work_bytes >= need) return AMA_OK;
   if (e->grid_work) cudaFree(e->grid_work);
   e->grid_work = nullptr;
@@ -1439,6 +1784,82 @@ extern "C" int ama_grid_fft_forward(AmaEngine* e, const double* in, void* out, v
   return AMA_OK;
 }
 
+namespace {
+Recip recip_of(const double* cell) {
+  // b_i = 2 pi (inverse of the cell matrix whose rows are a_1, a_2, a_3), transposed
+  const double* a = cell;
+  const double det = a[0] * (a[4] * a[8] - a[5] * a[7]) - a[1] * (a[3] * a[8] - a[5] * a[6]) +
+                     a[2] * (a[3] * a[7] - a[4] * a[6]);
+  const double f = 2.0 * M_PI / det;
+  Recip r;
+  // b_1 = 2 pi (a_2 x a_3) / det, and cyclically
+  const int nx[3][2] = {{1, 2}, {2, 0}, {0, 1}};
+  for (int i = 0; i < 3; ++i) {
+    const double* u = a + 3 * nx[i][0];
+    const double* v = a + 3 * nx[i][1];
+    r.b[i][0] = f * (u[1] * v[2] - u[2] * v[1]);
+    r.b[i][1] = f * (u[2] * v[0] - u[0] * v[2]);
+    r.b[i][2] = f * (u[0] * v[1] - u[1] * v[0]);
+  }
+  return r;
+}
+
+int grid_prepare(AmaEngine* e, int fields) {
+  AMA_REQUIRE(e->precisions & (1u << AMA_C128), AMA_ERR_ARG, "grid transforms need the complex128 tables");
+  if (int rc = require_engine_device(e)) return rc;
+  if (int rc = ensure_grid_work(e, fields)) return rc;
+  const size_t ps = plane_smem<double>(e), ss = slab_smem<double>(e);
+  AMA_CUDA_TRY(cudaFuncSetAttribute(grid_g1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
+  AMA_CUDA_TRY(cudaFuncSetAttribute(grid_g3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
+  AMA_CUDA_TRY(cudaFuncSetAttribute(grid_g3_axpy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
+  AMA_CUDA_TRY(cudaFuncSetAttribute(grid_g2_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
+  AMA_CUDA_TRY(cudaFuncSetAttribute(grid_g2_div_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
+  return AMA_OK;
+}
+}  // namespace
+
+extern "C" int ama_grid_gradient(AmaEngine* e, const double* cell, const double* in, double scale, double* out,
+                                 void* stream) {
+  AMA_REQUIRE(e && cell && in && out, AMA_ERR_ARG, "null argument");
+  if (int rc = grid_prepare(e, 4)) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  GridView g = grid_view(e);
+  const size_t ps = plane_smem<double>(e), ss = slab_smem<double>(e);
+  auto T = [&](int axis, int dir) { return (const double2*)e->d.tw[AMA_C128][axis][dir]; };
+  double2* w0 = e->grid_work;
+  double2* w1 = w0 + e->N;  // three outputs follow the G1 field
+  grid_g1_kernel<<<g.n1, kFftThreads, ps, s>>>(g, T(1, 1), T(2, 1), in, w0);
+  AMA_CHECK_LAUNCH();
+  grid_g2_grad_kernel<<<dim3(g.n2, 3), kFftThreads, ss, s>>>(g, T(0, 1), T(0, 0), recip_of(cell),
+                                                              scale / (double)e->N, w0, w1);
+  AMA_CHECK_LAUNCH();
+  for (int a = 0; a < 3; ++a) {
+    grid_g3_kernel<<<g.n1, kFftThreads, ps, s>>>(g, T(1, 0), T(2, 0), w1 + a * e->N, out + a * e->N);
+    AMA_CHECK_LAUNCH();
+  }
+  return AMA_OK;
+}
+
+extern "C" int ama_grid_divergence(AmaEngine* e, const double* cell, const double* in, double alpha, double beta,
+                                   double* out, void* stream) {
+  AMA_REQUIRE(e && cell && in && out, AMA_ERR_ARG, "null argument");
+  if (int rc = grid_prepare(e, 3)) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  GridView g = grid_view(e);
+  const size_t ps = plane_smem<double>(e), ss = slab_smem<double>(e);
+  auto T = [&](int axis, int dir) { return (const double2*)e->d.tw[AMA_C128][axis][dir]; };
+  double2* w = e->grid_work;
+  for (int a = 0; a < 3; ++a) {
+    grid_g1_kernel<<<g.n1, kFftThreads, ps, s>>>(g, T(1, 1), T(2, 1), in + a * e->N, w + a * e->N);
+    AMA_CHECK_LAUNCH();
+  }
+  grid_g2_div_kernel<<<g.n2, kFftThreads, ss, s>>>(g, T(0, 1), T(0, 0), recip_of(cell), 1.0 / (double)e->N, w);
+  AMA_CHECK_LAUNCH();
+  grid_g3_axpy_kernel<<<g.n1, kFftThreads, ps, s>>>(g, T(1, 0), T(2, 0), w, alpha, beta, out);
+  AMA_CHECK_LAUNCH();
+  return AMA_OK;
+}
+
 extern "C" int ama_engine_option(AmaEngine* e, int32_t option, int32_t value) {
   AMA_REQUIRE(e, AMA_ERR_ARG, "null engine");
   switch (option) {
@@ -1456,6 +1877,16 @@ extern "C" int ama_engine_option(AmaEngine* e, int32_t option, int32_t value) {
       e->stage_fn[p][1] = e->b_variant[p][value];
       e->regb[p] = value != 0;
       e->bthreads[p] = value == 3 ? 2 : 1;
+      return AMA_OK;
+    }
+    case 3: {  // complex64 stages A and C: 0 shared-memory y passes, 1 y in registers (4 lanes)
+      AMA_REQUIRE(e->precisions & (1u << AMA_C64), AMA_ERR_ARG, "the engine was created without complex64");
+      AMA_REQUIRE(value == 0 || value == 1, AMA_ERR_ARG, "stage A/C variant must be 0 or 1");
+      AMA_REQUIRE(e->ac_variant[AMA_C64][value][0] != nullptr, AMA_ERR_UNSUPPORTED,
+                  "this stage A/C variant is not compiled for the engine's grid");
+      e->stage_fn[AMA_C64][0] = e->ac_variant[AMA_C64][value][0];
+      e->stage_fn[AMA_C64][2] = e->ac_variant[AMA_C64][value][1];
+      e->ac_threads[AMA_C64] = e->ac_threads_of[AMA_C64][value];
       return AMA_OK;
     }
     default:

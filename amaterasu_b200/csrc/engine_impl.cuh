@@ -78,6 +78,9 @@ struct AmaEngine {
   bool regb[2] = {false, false};    // [prec] stage B with register-resident x columns
   const void* b_variant[2][4] = {};  // [prec] stage B variants compiled for the grid
   int bthreads[2] = {1, 1};          // [prec] threads per (y, z) column of the register stage B
+  const void* ac_variant[2][2][2] = {};  // [prec][variant][stage A, C] compiled for the grid
+  int ac_threads_of[2][2] = {};          // [prec][variant] threads per CTA of those stages
+  int ac_threads[2] = {256, 256};        // [prec] threads per CTA of the selected stages A and C
   NlTcState tc;
   bool use_tc = true;
   // FP64 grid transforms (Hartree, Kerker): reciprocal-space filters in the engine's

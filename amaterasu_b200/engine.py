@@ -134,6 +134,12 @@ class DeviceEngine:
         option = 1 if precision_code(precision) == AMA_C64 else 2
         call("ama_engine_option", self.handle, option, int(variant))
 
+    def set_stage_ac_variant(self, variant: int) -> None:
+        """Select the complex64 stages A and C (y and z transforms with the sphere scatter and
+        gather): 0 shared-memory y passes, 1 y transforms in registers with four lanes per
+        column. Raises NotImplementedError when the variant is not compiled for this grid."""
+        call("ama_engine_option", self.handle, 3, int(variant))
+
     def tc_status(self) -> int:
         code = ct.c_int32(0)
         call("ama_tc_status", self.handle, ct.byref(code))

@@ -1,9 +1,11 @@
 """Effective potential on the GPU in FP64: Hartree (reciprocal-space filter kernel),
-LDA-PZ exchange-correlation (pointwise kernel) and the local ionic potential.
+exchange-correlation (LDA-PZ pointwise kernel; PBE and PBEsol with spectral gradients and
+divergence) and the local ionic potential.
 
-Mirrors amaterasu ``scf/driver.py:330-357`` (``effective_potential``),
-``hamiltonian/hartree.py:28-50`` and ``xc/driver.py:108-164`` (LDA branch: the
-unpolarised density is split n/2, n/2 and the spin-polarised functional evaluated).
+Mirrors amaterasu ``scf/driver.py:225-252`` (``effective_potential``),
+``hamiltonian/hartree.py:28-50`` and ``xc/driver.py:108-165`` (the unpolarised density is
+split n/2, n/2 and the spin-polarised functional evaluated; a GGA adds
+-div(2 vsigma_ss grad n_s + vsigma_ud grad n_s') to the potential).
 """
 from __future__ import annotations
 
@@ -17,6 +19,18 @@ from .engine import engine_for, ptr, stream_ptr
 
 HARTREE_SLOT = 0
 KERKER_SLOT = 1
+#: functional name (as the reference spells it, case-insensitive) -> (kind, GGA code)
+FUNCTIONALS = {"LDA-PZ": ("lda", None), "PBE": ("gga", 0), "PBESOL": ("gga", 1)}
+
+
+def functional_key(name) -> str:
+    """Canonical key of a functional name or of an object with a ``name`` (the reference's
+    XCFunctional)."""
+    key = str(getattr(name, "name", name)).strip().upper().replace("_", "-")
+    if key not in FUNCTIONALS:
+        raise NotImplementedError(f"functional {name!r}: the engine implements "
+                                  f"{', '.join(('LDA-PZ', 'PBE', 'PBEsol'))}")
+    return key
 
 
 class GridOps:
@@ -84,6 +98,33 @@ class GridOps:
         call("ama_vec_reduce", 0, self.N, ptr(eps), ptr(total), float(self.dv), 0, ptr(energy), stream_ptr())
         return energy[0], vrho[:nspin]
 
+    def gga(self, density: torch.Tensor, functional: str = "PBE"):
+        """(E_xc device scalar, v_xc (nspin, N), gradient stress term (3, 3) device) for
+        density (nspin, N): PBE or PBEsol, gradients and divergence in reciprocal space.
+        The stress term is sum_r [2 vsigma_uu g_u g_u + vsigma_ud (g_u g_d + g_d g_u) +
+        2 vsigma_dd g_d g_d] dV (the reference subtracts it from the xc stress)."""
+        code = FUNCTIONALS[functional_key(functional)][1]
+        if code is None:
+            raise ValueError(f"{functional} is not a GGA")
+        d = density.reshape(density.shape[0], -1).to(self.device, torch.float64).contiguous()
+        nspin = d.shape[0]
+        v = torch.empty_like(d)
+        res = torch.empty(7, dtype=torch.float64, device=self.device)
+        cell = np.ascontiguousarray(self.grid.cell, dtype=np.float64)
+        call("ama_xc_gga", self.engine.handle, code, nspin, cell.ctypes.data_as(ct.c_void_p), ptr(d), ptr(v),
+             ptr(res), stream_ptr())
+        xx, yy, zz, yz, xz, xy = (res[i] for i in range(1, 7))
+        outer = torch.stack([torch.stack([xx, xy, xz]), torch.stack([xy, yy, yz]), torch.stack([xz, yz, zz])])
+        return res[0], v, outer
+
+    def xc(self, density: torch.Tensor, functional: str = "LDA-PZ"):
+        """(E_xc, v_xc (nspin, N), gradient stress term or None) for the system's functional."""
+        kind = FUNCTIONALS[functional_key(functional)][0]
+        if kind == "lda":
+            e, v = self.lda(density)
+            return e, v, None
+        return self.gga(density, functional)
+
 
 def grid_ops(system) -> GridOps:
     ops = getattr(system, "_grid_ops", None)
@@ -119,7 +160,7 @@ def effective_potential(system, density):
     if system.core_density is not None:
         core = torch.from_numpy(system.core_density.ravel()).to(ops.device)
         xc_density = d + core[None, :] / system.nspin
-    e_xc, v_xc = ops.lda(xc_density)
+    e_xc, v_xc, _ = ops.xc(xc_density, system.xc)
     vloc = getattr(system, "_v_local_dev", None)
     if vloc is None:
         vloc = torch.from_numpy(system.v_local.ravel()).to(ops.device)

@@ -139,8 +139,8 @@ def _xc_potential_mean(system, density):
     xc_d = d
     if system.core_density is not None:
         xc_d = d + torch.from_numpy(system.core_density.ravel()).to(d.device)[None] / system.nspin
-    e_xc, v_xc = ops.lda(xc_d)
-    return e_xc, v_xc, xc_d
+    e_xc, v_xc, outer = ops.xc(xc_d, system.xc)
+    return e_xc, v_xc, xc_d, outer
 
 
 def compute_forces(system, density, wavefunctions, occupations, *, eigenvalues=None, symmetrize=True,
@@ -161,7 +161,7 @@ def compute_forces(system, density, wavefunctions, occupations, *, eigenvalues=N
     out["local"] = local.cpu().numpy()
     out["nonlocal"] = _nonlocal_forces(system, wavefunctions, occupations, dev).cpu().numpy()
     if system.core_density is not None:
-        _, v_xc, _ = _xc_potential_mean(system, rho)
+        _, v_xc, _, _ = _xc_potential_mean(system, rho)
         v_g = density_coefficients(system, v_xc.mean(0))
         core = tabs.core()
         cf = torch.zeros((system.natoms, 3), dtype=torch.float64, device=dev)
@@ -289,10 +289,13 @@ def compute_stress(system, density, wavefunctions, occupations, *, eigenvalues=N
             tensor -= torch.einsum("g,gu,gv->uv", w, tabs.g, tabs.g)
     out["local"] = ((-torch.eye(3, device=dev, dtype=torch.float64) * energy + tensor) / vol).cpu().numpy()
     out["nonlocal"] = _nonlocal_stress(system, wavefunctions, occupations, dev)
-    # xc (LDA): delta_uv (E_xc - sum_s int v_xc^s n_s)
-    e_xc, v_xc, xc_d = _xc_potential_mean(system, rho)
+    # xc: delta_uv (E_xc - sum_s int v_xc^s n_s), minus the GGA gradient outer product
+    e_xc, v_xc, xc_d, outer = _xc_potential_mean(system, rho)
     dc = float((v_xc * xc_d).sum()) * system.grid.cell_volume_per_point
-    out["xc"] = np.eye(3) * (float(e_xc) - dc) / vol
+    xc_stress = np.eye(3) * (float(e_xc) - dc)
+    if outer is not None:
+        xc_stress = xc_stress - outer.cpu().numpy()
+    out["xc"] = xc_stress / vol
     if system.core_density is not None:
         v_g = density_coefficients(system, v_xc.mean(0))
         core_d = tabs.core(derivative=True)

@@ -318,7 +318,7 @@ def run_scf(system, config: Config | None = None, *, logger=None, wavefunctions=
         xc_d = rho_out
         if system.core_density is not None:
             xc_d = rho_out + torch.from_numpy(system.core_density.ravel()).to(dev)[None] / system.nspin
-        e_xc, _ = ops.lda(xc_d)
+        e_xc, _, _ = ops.xc(xc_d, system.xc)
         e_kin = _kinetic_energy(system, orb, occ, kin_packed)
         e_nl = _nonlocal_energy(system, orb, occ, dij_dev)
         if distributed:

@@ -65,9 +65,10 @@ TRAINING_SPACING_A = 5.43 / 36  # working-grid spacing the committed nets were t
 
 
 def run(workload: str, weights=None, forces=False, log=print, policies=("plain", "mixed", "learned+mixed"),
-        engine_options=None, spacing=TRAINING_SPACING_A, stress=False, hook=None) -> dict:
+        engine_options=None, spacing=TRAINING_SPACING_A, stress=False, hook=None, after=None) -> dict:
     """Run the policies on one system; ``hook(name, "start"|"stop")`` brackets each timed run
-    (the bench samples clocks there)."""
+    (the bench samples clocks there); ``after(system)``, when given, runs on the same system
+    once the policies are done and its result is returned under "after"."""
     import torch
     from .learned import DensityNet, LearnedStart, working_grid
     from .scf import prepare_starting_orbitals, run_scf
@@ -122,6 +123,8 @@ def run(workload: str, weights=None, forces=False, log=print, policies=("plain",
     for row in results.values():
         row.pop("_forces", None)
         row.pop("_stress", None)
+    if after is not None:
+        out["after"] = after(system)
     return out
 
 

@@ -114,8 +114,8 @@ def build_system(atoms, pseudopotentials: dict, ecut: float, ecut_rho: float | N
                  nspin: int = 1, xc: str = "LDA-PZ", charge: float = 0.0,
                  build_projector_matrices: bool = True) -> PlaneWaveSystem:
     """Assemble the fixed part of a calculation; ``ecut``/``ecut_rho`` in Hartree."""
-    if xc.upper() != "LDA-PZ":
-        raise NotImplementedError(f"functional {xc!r}: only LDA-PZ is implemented")
+    from .potential import functional_key
+    xc = {"LDA-PZ": "LDA-PZ", "PBE": "PBE", "PBESOL": "PBEsol"}[functional_key(xc)]
     ecut_rho = 4.0 * ecut if ecut_rho is None else ecut_rho
     symbols, pos_ang, cell_ang = _structure_arrays(atoms)
     cell = cell_ang * ANG_IN_BOHR

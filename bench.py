@@ -47,6 +47,8 @@ METRIC = "Hpsi bands/s (Si64 40 Ry 84^3, 4 k x 160 bands)"
 # ncu DRAM bytes of one all-k call, written by the profiling recipe in profiles/ together with
 # a hash of the CUDA sources they were measured on; used only while the sources match
 TRAFFIC_FILE = REPO / "profiles" / "hpsi_si64_traffic.json"
+HPSI_SOURCES = ("common.cuh", "dft.cuh", "twiddles.h", "twiddles_line.h", "engine_impl.cuh", "engine.cu",
+                "gemm.cuh", "nl_tc.cu", "tc_chain.cuh", "tc_gemm.cuh")
 
 
 def parse():
@@ -60,6 +62,9 @@ def parse():
     ap.add_argument("--kpoints", type=int, default=4, help="k-points of the workload to include (profiling)")
     ap.add_argument("--no-extras", action="store_true", help="skip the e2e and complex128 legs (profiling)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the engine's default kernel variants")
+    ap.add_argument("--variants", default=None, metavar="B,AC,TC",
+                    help="force the complex64 kernel variants (stage B, stages A/C, tensor-core nonlocal 0/1) "
+                         "instead of timing them: profiling runs reproduce a timed run's choice with it")
     ap.add_argument("--no-scf", action="store_true",
                     help="skip the Si215 Gamma SCF block (plain FP64, mixed, learned+mixed; ~2 minutes)")
     ap.add_argument("--density-only", action="store_true",
@@ -70,11 +75,13 @@ def parse():
 
 
 def source_hash() -> str:
-    """SHA-256 of the CUDA sources (what a DRAM-traffic measurement belongs to)."""
+    """SHA-256 of the CUDA sources the H.psi call compiles from (what a DRAM-traffic
+    measurement belongs to)."""
     import hashlib
     h = hashlib.sha256()
-    for p in sorted((REPO / "amaterasu_b200" / "csrc").glob("*")):
-        h.update(p.name.encode())
+    for name in HPSI_SOURCES:
+        p = REPO / "amaterasu_b200" / "csrc" / name
+        h.update(name.encode())
         h.update(p.read_bytes())
     return h.hexdigest()[:16]
 
@@ -323,7 +330,13 @@ def hpsi_leg(system, veff, blocks, nbands, prec, steps, warmup, stream, autotune
     psi = torch.from_numpy(host).cuda()
     out = torch.empty_like(psi)
     eng.reserve(prec, nk * nbands)
-    if autotune:
+    if isinstance(autotune, tuple) and prec == "complex64":
+        b, ac, tc = autotune
+        eng.set_stage_b_variant(prec, b)
+        eng.set_stage_ac_variant(ac)
+        eng.set_tensor_core_nonlocal(bool(tc))
+        tuned = {"stage_b": b, "stage_ac": ac, "nonlocal_tc": bool(tc), "forced": True}
+    elif autotune:
         from amaterasu_b200.autotune import autotune_hpsi
         tuned = autotune_hpsi(H, nbands)
     else:
@@ -401,8 +414,44 @@ def density_leg(system, blocks, nbands, steps, stream, peak):
     return out
 
 
-def scf_block(log=lambda *_: None):
-    """Si215 SCF policies with a clock record per policy."""
+def hpsi_config5(system, peak, steps=10):
+    """H.psi of the Si215 Gamma configuration (108^3 grid, 440 bands, 80,797 plane waves)
+    in both precisions on the SCF's own system: device-timed all-band calls after the
+    kernel-variant autotune, with the roofline on the algorithmic bytes and the measured
+    copy bandwidth."""
+    import torch
+    from amaterasu_b200.autotune import autotune_hpsi
+    from amaterasu_b200.hamiltonian import Hamiltonian
+    from amaterasu_b200.potential import effective_potential
+    nb = int(system.nbands)
+    veff, _, _ = effective_potential(system, system.initial_density())
+    veff = veff.cpu().numpy()
+    w = system.wave_spheres[0]
+    rng = np.random.default_rng(5)
+    block = (rng.normal(size=(nb, len(w))) + 1j * rng.normal(size=(nb, len(w)))) / (1.0 + w.kinetic_energy)
+    stream = torch.cuda.current_stream()
+    out = {"workload": "si215_gamma", "bands": nb, "plane_waves": len(w), "grid": list(system.grid.shape)}
+    for prec, itemsize in (("complex64", 8), ("complex128", 16)):
+        H = Hamiltonian(system, veff, precision=prec)
+        psi = torch.from_numpy(block.astype(np.complex64 if prec == "complex64" else np.complex128).ravel()).cuda()
+        res = torch.empty_like(psi)
+        tuned = autotune_hpsi(H, nb)
+        for _ in range(3):
+            H.apply_all(psi, nb, out=res)
+        torch.cuda.synchronize()
+        ms = time_calls(lambda: H.apply_all(psi, nb, out=res), steps, stream) / steps
+        alg = algorithmic_bytes(system, nb, itemsize)
+        achieved = alg / (ms / 1e3) / 1e9
+        out[prec] = {"ms_per_call": ms, "bands_per_s": nb / (ms / 1e3),
+                     "autotune": {k: tuned[k] for k in ("stage_b", "stage_ac", "nonlocal_tc") if k in tuned},
+                     "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak["value"], "unit": "GB/s",
+                                  "frac": achieved / peak["value"], "algorithmic_bytes": alg,
+                                  "peak_source": peak["source"]}}
+    return out
+
+
+def scf_block(log=lambda *_: None, peak=None):
+    """Si215 SCF policies with a clock record per policy, then the Si215 H.psi figures."""
     from amaterasu_b200.scf_benchmark import run as scf_run
     weights = REPO / "amaterasu_b200" / "data" / "density_net_si64.npz"
     samplers = {}
@@ -415,7 +464,11 @@ def scf_block(log=lambda *_: None):
         else:
             samplers[name] = samplers[name].stop(samplers[name]._first)
 
-    out = scf_run("si215_gamma", str(weights) if weights.exists() else None, forces=True, log=log, hook=hook)
+    after = (lambda system: hpsi_config5(system, peak)) if peak is not None else None
+    out = scf_run("si215_gamma", str(weights) if weights.exists() else None, forces=True, log=log, hook=hook,
+                  after=after)
+    if "after" in out:
+        out["hpsi_config5"] = out.pop("after")
     for name, row in out["runs"].items():
         row["clocks"] = samplers.get(name)
     plain, best = out["runs"].get("plain"), out["runs"].get("learned+mixed") or out["runs"].get("mixed")
@@ -472,8 +525,9 @@ def main():
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
+    tune = tuple(int(x) for x in args.variants.split(",")) if args.variants else not args.no_autotune
     main_rec, out_np, host = hpsi_leg(system, veff, blocks, nbands, prec, args.steps, args.warmup, stream,
-                                      not args.no_autotune, not args.no_extras, peak)
+                                      tune, not args.no_extras, peak)
     clocks = sampler.stop(first_sample)
 
     t = torch.tensor([main_rec["ms"], main_rec["e2e_ms"]], dtype=torch.float64, device="cuda")
@@ -508,7 +562,7 @@ def main():
         "scaling": "weak", "vs_baseline": None, "dtype": "c64" if prec == "complex64" else "c128",
         "data": "synthetic",
         "config": {**_common_config(system, nbands), "parallelism": f"replicas x{world}"},
-        "autotune": {"stage_b": main_rec["tuned"]["stage_b"], "nonlocal_tc": main_rec["tuned"]["nonlocal_tc"]},
+        "autotune": {k: main_rec["tuned"][k] for k in ("stage_b", "stage_ac", "nonlocal_tc") if k in main_rec["tuned"]},
         "roofline": main_rec["roofline"],
         "e2e": {"value": e2e_value, "unit": "bands/s",
                 "h2d_bytes_per_step": main_rec["bytes"], "d2h_bytes_per_step": main_rec["bytes"]},
@@ -528,7 +582,7 @@ def main():
                                 "sample": f"{done} bands (8-band blocks cycling over the 4 k-points, {elapsed:.1f} s), "
                                           f"oracle FP64 H.psi, scipy.fft workers={threads}, BLAS {threads} threads"}
     if world == 1 and not args.no_scf:
-        line["scf"] = scf_block()
+        line["scf"] = scf_block(peak=peak)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

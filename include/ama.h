@@ -74,6 +74,10 @@ AMA_API int ama_engine_destroy(AmaEngine* engine);
  *             x-plane set, 3 register-resident with two threads per column (even x length);
  *             AMA_ERR_UNSUPPORTED when the variant is not compiled for the grid;
  *   option 2: the same for complex128 (only variant 0 exists).
+ *   option 3: complex64 stages A and C (scatter + z, y backward; y, z forward + gather)
+ *             variant: 0 shared-memory y passes, 1 y transforms in registers with four
+ *             threads per column (n2 a multiple of 4 on a compile-time grid);
+ *             AMA_ERR_UNSUPPORTED when the variant is not compiled for the grid.
  * amaterasu_b200.autotune times the variants and keeps the fastest. */
 AMA_API int ama_engine_option(AmaEngine* engine, int32_t option, int32_t value);
 
@@ -200,6 +204,30 @@ AMA_API int ama_grid_filter_noalloc(AmaEngine* engine, int32_t slot, int32_t ene
  * [n1*n2*n3], device complex128 out [n1*n2*n3]): out[G] = (1/N) sum_r in(r) e^{-iG.r}.
  * Replaces FFTGrid.to_reciprocal on a density (basis/fft.py:228-235). */
 AMA_API int ama_grid_fft_forward(AmaEngine* engine, const double* in, void* out, void* stream);
+
+/* Spectral gradient of a real grid field (device FP64 in [N], out [3][N], Cartesian x, y, z):
+ * out_a = scale * Re IFFT(i G_a FFT(in)), the Nyquist frequency of every even axis zeroed.
+ * cell: host, the 3 x 3 lattice vectors as rows (Bohr). Needs the complex128 tables.
+ * Replaces FFTGrid.gradient (basis/fft.py:288-295). */
+AMA_API int ama_grid_gradient(AmaEngine* engine, const double* cell, const double* in, double scale,
+                              double* out, void* stream);
+
+/* Spectral divergence of a real vector field (device FP64 in [3][N]), accumulated:
+ * out = beta * out + alpha * Re IFFT(sum_a i G_a FFT(in_a)) (Nyquist zeroed as above).
+ * Replaces FFTGrid.divergence (basis/fft.py:297-304). */
+AMA_API int ama_grid_divergence(AmaEngine* engine, const double* cell, const double* in, double alpha,
+                                double beta, double* out, void* stream);
+
+/* PBE (functional 0) or PBEsol (1) exchange-correlation of a density (device FP64
+ * rho [nspin][N], electrons/Bohr^3; nspin 1 is split n/2, n/2): vxc [nspin][N] the full
+ * potential d(n eps)/dn_s - div(2 vsigma_ss grad n_s + vsigma_ud grad n_s'); result (device,
+ * 7 doubles): [0] E_xc (Ha), [1..6] the gradient stress sum
+ * sum_r [2 vsigma_uu g_u g_u + vsigma_ud (g_u g_d + g_d g_u) + 2 vsigma_dd g_d g_d] dV in the
+ * order xx yy zz yz xz xy. Replaces XCFunctional.evaluate_on_grid for a GGA
+ * (xc/driver.py:108-165, xc/gga.py:112-254) and the gradient part of the xc stress
+ * (properties/stress.py:159-185). */
+AMA_API int ama_xc_gga(AmaEngine* engine, int32_t functional, int32_t nspin, const double* cell,
+                       const double* rho, double* vxc, double* result, void* stream);
 
 /* ama_residual_precondition for every k-point in one launch: x/hx packed (nbands, npw_k)
  * blocks, eps/norms [nk][nbands], kinetic packed by pw_off; rows [nk][nbands] gives the

@@ -21,6 +21,9 @@ Fixtures (``*.npz``):
   si215.npz     Si215 (3x3x3 conventional, one vacancy, displaced), Gamma, 30 Ry, 440
                 bands: sphere and projector pins, Ewald energy/forces/stress, v_eff
                 checksums and probes, starting-orbital pins, H.psi of a few bands
+  gga.npz       PBE / PBEsol: pointwise outputs at seeded points, the grid functional on
+                the mini system's start density (unpolarised and spin-split), and a Si2
+                PBE SCF (20 Ry, shifted 2x2x2, 8 bands) with forces and stress
 """
 from __future__ import annotations
 
@@ -350,6 +353,69 @@ def make_si215(pseudo, out):
     np.savez_compressed(out / "si215.npz", **d)
 
 
+# ------------------------------------------------------------------------------ gga
+def make_gga(pseudo, out):
+    """PBE / PBEsol: the pointwise functionals at seeded points, the grid functional on the
+    mini system's starting density (unpolarised, and split 0.6 / 0.4 between the spins), and
+    a small Si2 PBE SCF with forces and stress."""
+    from amaterasu.properties.forces import compute_forces
+    from amaterasu.properties.stress import compute_stress
+    from amaterasu.scf.driver import run_scf
+    from amaterasu.xc import gga
+    from amaterasu.xc.driver import XCFunctional
+    from amaterasu_b200.cells import si2_primitive
+
+    rng = np.random.default_rng(2024)
+    n = 600
+    tot = 10.0 ** rng.uniform(-6, 1, n)
+    zeta = rng.uniform(-0.95, 0.95, n)
+    zeta[:100] = 0.0
+    rho = np.stack([tot * (1 + zeta) / 2, tot * (1 - zeta) / 2], axis=-1)
+    g = rng.normal(size=(n, 2, 3)) * tot[:, None, None] ** (4 / 3) * 10.0 ** rng.uniform(-3, 1, (n, 1, 1))
+    g[:40] = 0.0
+    sigma = np.stack([np.sum(g[:, 0] * g[:, 0], 1), np.sum(g[:, 0] * g[:, 1], 1), np.sum(g[:, 1] * g[:, 1], 1)], -1)
+    d = dict(rho=rho, sigma=sigma)
+    for name in ("PBE", "PBEsol"):
+        ex, vx, sx = gga.exchange(rho, sigma, name)
+        ec, vc, sc = gga.correlation(rho, sigma, name)
+        d[f"{name}_eps"] = ex + ec
+        d[f"{name}_vrho"] = vx + vc
+        d[f"{name}_vsigma"] = sx + sc
+    system = reference_mini_system()
+    rho0 = system.initial_density()
+    d["mini_cell"] = system.grid.cell
+    d["mini_rho0"] = rho0
+    for name in ("PBE", "PBEsol"):
+        r = XCFunctional(name).evaluate_on_grid(rho0, system.grid)
+        d[f"mini_{name}_energy"] = r.energy
+        d[f"mini_{name}_potential"] = r.potential
+    pol = np.stack([0.6 * rho0[0], 0.4 * rho0[0]])
+    r = XCFunctional("PBE").evaluate_on_grid(pol, system.grid)
+    d["mini_pol_energy"] = r.energy
+    d["mini_pol_potential"] = r.potential
+    cfg = _config(kpoints__grid=[2, 2, 2], kpoints__shift=[0.5, 0.5, 0.5], occupations__scheme="fixed",
+                  occupations__nbands=8, scf__tol_energy=1e-8, scf__tol_density=1e-8)
+    cfg.xc.functional = "PBE"
+    system = _system(si2_primitive(), cfg, pseudo, 10.0)
+    result = run_scf(system, cfg, logger=print)
+    forces = compute_forces(system, result.density, result.wavefunctions, result.occupations,
+                            eigenvalues=result.eigenvalues, decompose=True)
+    stress = compute_stress(system, result.density, result.wavefunctions, result.occupations,
+                            eigenvalues=result.eigenvalues, decompose=True)
+    e = result.energies
+    d.update(scf_grid=np.array(system.grid.shape), scf_kpoints=system.kpoints.points,
+             scf_weights=system.kpoints.weights, scf_iterations=result.iterations,
+             scf_converged=result.converged, scf_e_kinetic=e.kinetic, scf_e_local=e.local,
+             scf_e_hartree=e.hartree, scf_e_xc=e.xc, scf_e_nonlocal=e.nonlocal_, scf_e_ewald=e.ewald,
+             scf_e_total=e.total, scf_e_free=e.free_energy, scf_eigenvalues=result.eigenvalues,
+             scf_density=result.density)
+    for name, value in forces.items():
+        d[f"scf_force_{name}"] = value
+    for name, value in stress.items():
+        d[f"scf_stress_{name}"] = value
+    np.savez_compressed(out / "gga.npz", **d)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=DEFAULT_REFERENCE)
@@ -357,7 +423,7 @@ def main():
     args = ap.parse_args()
     _import_reference(args.reference)
     jobs = {"mini": make_mini, "si8": make_si8, "si64": make_si64, "si2": make_si2,
-            "si215": make_si215, "si8_scf1": make_si8_scf1}
+            "si215": make_si215, "si8_scf1": make_si8_scf1, "gga": make_gga}
     with tempfile.TemporaryDirectory() as tmp:
         pseudo, _ = _upf(tmp)
         for name, job in jobs.items():

@@ -27,6 +27,17 @@ def _available(eng, precision):
     return out
 
 
+def _available_ac(eng):
+    out = []
+    for v in (0, 1):
+        try:
+            eng.set_stage_ac_variant(v)
+            out.append(v)
+        except NotImplementedError:
+            pass
+    return out
+
+
 @pytest.mark.parametrize("precision,tol", [("complex128", 1e-11), ("complex64", 2e-5)])
 def test_every_variant_matches_the_oracle(mini_system, precision, tol):
     from amaterasu_b200.autotune import autotune_hpsi
@@ -70,14 +81,44 @@ def test_si64_variants_match_the_reference(si_pseudo):
     eng = H.engine
     variants = _available(eng, "complex64")
     assert variants == [0, 1, 2, 3]
+    ac = _available_ac(eng)
+    assert ac == [0, 1]
     for v in variants:
         eng.set_stage_b_variant("complex64", v)
-        for ik, nbk in ((0, 2), (1, 1)):
-            w = s.wave_spheres[ik]
-            rng = np.random.default_rng(300 + ik)
-            psi = (rng.normal(size=(nbk, len(w))) + 1j * rng.normal(size=(nbk, len(w)))) / (1.0 + w.kinetic_energy)
-            assert _rel(H.apply(psi, ik), g[f"hpsi{ik}"]) < 2e-5, (v, ik)
+        for a in ac:
+            eng.set_stage_ac_variant(a)
+            for ik, nbk in ((0, 2), (1, 1)):
+                w = s.wave_spheres[ik]
+                rng = np.random.default_rng(300 + ik)
+                psi = (rng.normal(size=(nbk, len(w))) + 1j * rng.normal(size=(nbk, len(w)))) / (1.0 + w.kinetic_energy)
+                assert _rel(H.apply(psi, ik), g[f"hpsi{ik}"]) < 2e-5, (v, a, ik)
     choice = autotune_hpsi(H, 32)
     print("autotune", choice)
-    assert choice["stage_b"] in variants
+    assert choice["stage_b"] in variants and choice["stage_ac"] in ac
     torch.cuda.synchronize()
+
+
+def test_si8_grid_variants_match_the_oracle(si_pseudo):
+    """42^3 grid (the 260-k Si8 configuration's): every stage B variant, on two k-points of
+    its mesh with 20 bands, against the oracle's FP64 H.psi."""
+    from amaterasu_b200 import kpoints as kp
+    from amaterasu_b200.cells import workload
+    from amaterasu_b200.hamiltonian import Hamiltonian
+    from amaterasu_b200.system import build_system
+    structure, ecut, ks, nb = workload("si8_batched")
+    two = kp.KPointSet(ks.points[[0, 37]], ks.weights[[0, 37]], ks.mesh, ks.shift)
+    s = build_system(structure, {"Si": si_pseudo}, ecut, 4 * ecut, kpoints=two, nbands=nb)
+    assert tuple(s.grid.shape) == (42, 42, 42)
+    rng = np.random.default_rng(42)
+    veff = rng.normal(size=(1, *s.grid.shape))
+    H = Hamiltonian(s, veff, precision="complex64")
+    eng = H.engine
+    variants = _available(eng, "complex64")
+    assert variants == [0, 1, 3]
+    for v in variants:
+        eng.set_stage_b_variant("complex64", v)
+        for ik, w in enumerate(s.wave_spheres):
+            psi = (rng.normal(size=(nb, len(w))) + 1j * rng.normal(size=(nb, len(w)))) / (1.0 + w.kinetic_energy)
+            ref = hamiltonian_apply(psi, w.miller, s.grid.shape, w.kinetic_energy, veff[0],
+                                    s.projectors[ik].matrix, s.projectors[ik].dij)
+            assert _rel(H.apply(psi, ik), ref) < 2e-5, (v, ik)

@@ -120,7 +120,7 @@ def test_si215_hpsi_matches_reference(si215_system, precision, tol):
     rng = np.random.default_rng(2150)
     psi = (rng.normal(size=(3, len(sphere))) + 1j * rng.normal(size=(3, len(sphere)))) / (1.0 + sphere.kinetic_energy)
     assert _rel(H.apply(psi, 0), g["hpsi"]) < tol
-    if precision == "complex64":  # every stage B variant compiled for the 108^3 grid
+    if precision == "complex64":  # every stage B x stage A/C variant compiled for the 108^3 grid
         variants = []
         for v in (0, 1, 2, 3):
             try:
@@ -128,9 +128,12 @@ def test_si215_hpsi_matches_reference(si215_system, precision, tol):
             except NotImplementedError:
                 continue
             variants.append(v)
-            assert _rel(H.apply(psi, 0), g["hpsi"]) < tol, v
+            for a in (0, 1):
+                H.engine.set_stage_ac_variant(a)
+                assert _rel(H.apply(psi, 0), g["hpsi"]) < tol, (v, a)
         assert variants == [0, 3]
         H.engine.set_stage_b_variant(precision, 0)
+        H.engine.set_stage_ac_variant(0)
 
 
 # ------------------------------------------------------------------------- Si8, 260 k-points
