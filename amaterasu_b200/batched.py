@@ -6,7 +6,9 @@ projections off the basis, drop directions below 1e-7, orthonormalise, extend, c
 subspace_factor * nbands). All k-points advance together: every step is one launch over all
 k (ragged plane-wave counts), H.psi runs on every k's new block in one engine call, the
 small per-k problems are solved by the batched Jacobi eigensolver, and the host synchronises
-three times per iteration for the whole set instead of per k.
+three times per iteration for the whole set instead of per k. ``BatchedDavidson.run`` runs
+the loop inside the library (``ama_davidson``, csrc/davidson.cu); ``run_python`` is the same
+loop with its host logic written here over the same kernels, kept as its check.
 
 Storage: the basis of k-point k is a (cap, npw_k) block at cap * pw_off[k]; every k carries
 the same number of rows. When a k-point has fewer new directions than the others (fewer
@@ -64,6 +66,7 @@ class BatchedDavidson:
         # complex64 plane-wave products on the tensor cores (split-TF32) once the spheres are
         # long enough for the staged tiles to pay; shorter ones stay on the SIMT kernels
         self.tensor_cores = bool(tensor_cores) and dtype == torch.complex64 and self.max_npw >= tc_min_npw
+        self.tc_min_npw = int(tc_min_npw)
         self.trace = []  # per iteration of the last run: (iteration, active directions, subspace size, max norm)
 
     # ---------------------------------------------------------------- kernels
@@ -200,8 +203,24 @@ class BatchedDavidson:
 
     # -------------------------------------------------------------------- run
     def run(self, H, guess_packed: torch.Tensor, *, tolerance=1e-8, max_iterations=40, spin=0):
-        """Lowest nbands eigenpairs at every k. ``guess_packed`` packs one (nbands, npw_k)
-        block per k; returns (eigenvalues [nk][nb] numpy, X packed, norms numpy, iterations)."""
+        """Lowest nbands eigenpairs at every k through the library's own loop
+        (``ama_davidson``: the iteration below, orchestrated in C++). ``guess_packed`` packs
+        one (nbands, npw_k) block per k; returns (eigenvalues [nk][nb] numpy, X packed,
+        norms numpy, iterations)."""
+        H._bind()
+        guess = guess_packed.to(self.dtype).contiguous()
+        eps = torch.empty((self.nk, self.nb), dtype=torch.float64, device=self.dev)
+        norms = torch.empty_like(eps)
+        X = torch.empty_like(guess)
+        it = ct.c_int32(0)
+        tc_min = self.tc_min_npw if self.tensor_cores else 0
+        call("ama_davidson", self.eng.handle, self.prec, int(spin), self.nb, ptr(guess), float(tolerance),
+             int(max_iterations), int(tc_min), ptr(eps), ptr(X), ptr(norms), ct.byref(it), stream_ptr())
+        return eps.cpu().numpy(), X, norms.cpu().numpy(), int(it.value)
+
+    def run_python(self, H, guess_packed: torch.Tensor, *, tolerance=1e-8, max_iterations=40, spin=0):
+        """The same iteration with its host logic in Python over the same kernels; kept to
+        check ``ama_davidson`` against (tests/test_eigen_gpu.py). Records ``trace``."""
         nb, cap = self.nb, self.cap
         self.trace = []
         H._bind()

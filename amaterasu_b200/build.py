@@ -13,7 +13,7 @@ HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 LIB = HERE / "libama.so"
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
-SOURCES = ["api.cu", "engine.cu", "nl_tc.cu", "subspace_tc.cu", "gemm_api.cu", "vecops.cu", "eig.cu", "hermitian.cu", "ewald.cu", "gridvec.cu", "xc_gga.cu",
+SOURCES = ["api.cu", "engine.cu", "nl_tc.cu", "subspace_tc.cu", "gemm_api.cu", "vecops.cu", "eig.cu", "hermitian.cu", "ewald.cu", "gridvec.cu", "xc_gga.cu", "davidson.cu",
            "convnet.cu"]
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",

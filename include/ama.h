@@ -237,6 +237,21 @@ AMA_API int ama_kbatch_residual(int32_t precision, int32_t nk, int32_t nbands, c
                                 const double* kinetic, double* norms, const int32_t* rows, int32_t nrows,
                                 void* out, void* stream);
 
+/* Block Davidson for the nbands lowest eigenpairs at every k-point of the engine, all
+ * k-points in lockstep, with the engine's H.psi (its current potential, spin channel
+ * `spin`) as the operator; the reference's algorithm per k-point (scf/eigen/davidson.py:48-111:
+ * Rayleigh-Ritz, Teter-Payne-Allan corrections of the bands with residual norm > tolerance,
+ * two projections off the basis, 1e-7 rank test, orthonormalisation, collapse at 4 nbands),
+ * orchestrated in C++ over the library's kernels. guess and x: device, one row-major
+ * (nbands, npw_k) block per k-point back to back, in the precision's complex type (x may be
+ * guess). eigenvalues, norms: device FP64 [nk][nbands] (norms may be NULL); iterations: host.
+ * tc_min_npw > 0 routes the complex64 plane-wave products to the tensor cores when the
+ * largest sphere has at least that many plane waves (0: never). The host synchronises three
+ * times per iteration. AMA_ERR_ARG for a rank-deficient start. */
+AMA_API int ama_davidson(AmaEngine* engine, int32_t precision, int32_t spin, int32_t nbands, const void* guess,
+                         double tolerance, int32_t max_iterations, int32_t tc_min_npw, double* eigenvalues,
+                         void* x, double* norms, int32_t* iterations, void* stream);
+
 /* Copy nrows rows per k-point between packed per-k blocks (block k at rows_per_k*pw_off[k],
  * rows of npw_k elements, starting at row row0). */
 AMA_API int ama_kbatch_copy_rows(int32_t precision, int32_t nk, int32_t nrows, const int32_t* npw,

