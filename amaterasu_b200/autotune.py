@@ -3,7 +3,8 @@
 The engine compiles several variants of the x-transform stage ("stage B": shared-memory
 slabs; register-resident x columns for short x lines; register-resident with the spheres'
 x-plane set fixed at compile time, for the benchmark grid; register-resident with two
-threads per column, for even x lengths up to 108), two variants of the stages around it
+threads per column, for even x lengths up to 108; shared-memory slabs split in two along z,
+for the long lines of a 108^3 grid), two variants of the stages around it
 (y transforms in shared memory or in registers with four lanes per column) and two paths
 for the complex64 nonlocal products (tcgen05 split-TF32 GEMMs or SIMT GEMMs). Which is fastest depends on the
 grid, the band count and the number of k-points of a call. ``autotune_hpsi`` times every
@@ -22,7 +23,7 @@ from .engine import TORCH_DTYPE, precision_code
 def _variants(eng, prec_code):
     """Stage B variants the engine has for this precision (probe by selecting them)."""
     out = []
-    for v in (0, 1, 2, 3):
+    for v in (0, 1, 2, 3, 4):
         try:
             eng.set_stage_b_variant(prec_code, v)
             out.append(v)

@@ -71,6 +71,11 @@ class EngineConfig:
     # lowest Davidson residual tolerance of the complex64 iterations: the FP32 H.psi and
     # subspace products leave a residual noise of a few 1e-7 Ha
     c64_tolerance_floor: float = 2e-6
+    # highest Davidson residual tolerance of the complex64 iterations (1e-3 of the density
+    # residual up to this; the reference's schedule caps at 1e-6): while the density is far
+    # from converged its eigenpairs need not be tighter (measured on Si215: same fixed point,
+    # 11% less time than with the 1e-6 cap)
+    c64_tolerance_cap: float = 1e-4
     # Davidson iterations per SCF step once a mixed run has switched to complex128 (0: the
     # reference's 20); the orbitals enter the refinement converged to the FP32 floor, and
     # the SCF convergence test is unchanged

@@ -102,11 +102,11 @@ struct DynDims {
   template <class V> __device__ static __forceinline__ int n3(const V& v) { return v.n3; }
   template <class V> __device__ static __forceinline__ int a3(const V& v) { return v.A3; }
 };
-template <int N1, int A1, int N2, int A2, int N3, int A3> struct FixDims {
+template <int N1, int A1, int N2, int A2, int N3, int A3, int ZS = 1> struct FixDims {
   static constexpr int n3c() { return N3; }
-  // stage B may split each (x, z) slab into z parts (less shared memory per CTA); measured
-  // slower at the benchmark grids, so one part
-  static constexpr int zsplit = 1;
+  // stage B may split each (x, z) slab into ZS parts along z (less shared memory per CTA,
+  // more CTAs per SM); one part by default, the split is an autotuned variant
+  static constexpr int zsplit = ZS;
   template <class V> __device__ static constexpr int n1(const V&) { return N1; }
   template <class V> __device__ static constexpr int a1(const V&) { return A1; }
   template <class V> __device__ static constexpr int n2(const V&) { return N2; }
@@ -755,13 +755,15 @@ density_b_kernel(HpsiView v, const cx_t<T>* __restrict__ tw_xb, const cx_t<T>* _
 
 // The stage B variants compiled for a grid: [0] shared-memory slab, [1] register-resident
 // x columns, [2] register-resident with the compile-time slot set, [3] register-resident
-// with two threads per column (null when absent).
+// with two threads per column, [4] shared-memory slab split in two along z (null when
+// absent), with the z split of each.
 // The stage A/C pairs: [0] shared-memory y passes, [1] y transforms in registers with four
 // lanes per column (null when absent), with their threads per CTA.
 struct StageInfo {
   int zsplit;
   bool regb;
-  const void* b_variant[4];
+  const void* b_variant[5];
+  int b_zsplit[5] = {1, 1, 1, 1, 2};
   const void* ac_variant[2][2] = {};
   int ac_threads[2] = {kFftThreads, kFftThreads};
 };
@@ -772,7 +774,7 @@ StageInfo fill_stage_table(const void** fn) {
   fn[1] = (const void*)stage_b_kernel<T, D>;
   fn[2] = (const void*)stage_c_kernel<T, D>;
   fn[3] = (const void*)density_b_kernel<T, D>;
-  StageInfo info{D::zsplit, false, {fn[1], nullptr, nullptr}};
+  StageInfo info{D::zsplit, false, {fn[1], nullptr, nullptr, nullptr, nullptr}};
   info.ac_variant[0][0] = fn[0];
   info.ac_variant[0][1] = fn[2];
   return info;
@@ -804,6 +806,15 @@ void add_pair_variant(StageInfo& info) {
       info.b_variant[3] = (const void*)stage_b_pair_kernel<N1, AH, D>;
     }
   }
+}
+
+// the shared-memory stage B with each (x, z) slab split in two along z, for long lines
+// (the whole-slab CTA of a 108^3 grid holds 93 KB (complex64) or 186 KB (complex128) of
+// shared memory, which leaves one or two CTAs per SM)
+template <typename T, int N1, int A1, int N2, int A2, int N3, int A3>
+void add_zsplit_variant(StageInfo& info) {
+  if constexpr (N3 % 2 == 0 && N1 >= 100)
+    info.b_variant[4] = (const void*)stage_b_kernel<T, FixDims<N1, A1, N2, A2, N3, A3, 2>>;
 }
 
 // complex64 on a compile-time grid with short x columns: register-resident stage B
@@ -840,9 +851,12 @@ StageInfo select_stage_table(const AxisPlan* ax, const void** fn, int hp, int hn
       StageInfo info = fill_stage_table<T, D>(fn);                                               \
       add_pair_variant<N1, D>(info);                                                             \
       add_quad_variant<N2, D>(info);                                                             \
+      add_zsplit_variant<T, N1, A1, N2, A2, N3, A3>(info);                                       \
       return info;                                                                               \
     } else {                                                                                     \
-      return fill_stage_table<T, D>(fn);                                                         \
+      StageInfo info = fill_stage_table<T, D>(fn);                                               \
+      add_zsplit_variant<T, N1, A1, N2, A2, N3, A3>(info);                                       \
+      return info;                                                                               \
     }                                                                                            \
   }
   AMA_FIX(20, 5, 20, 5, 20, 5)
@@ -969,7 +983,14 @@ int set_smem_limits(const AmaEngine* e) {
   const_cast<AmaEngine*>(e)->zsplit[p] = info.zsplit;
   const_cast<AmaEngine*>(e)->regb[p] = info.regb;
   const_cast<AmaEngine*>(e)->bthreads[p] = 1;
-  for (int i = 0; i < 4; ++i) const_cast<AmaEngine*>(e)->b_variant[p][i] = info.b_variant[i];
+  for (int i = 0; i < 5; ++i) {
+    const_cast<AmaEngine*>(e)->b_variant[p][i] = info.b_variant[i];
+    const_cast<AmaEngine*>(e)->b_zsplit[p][i] = info.b_zsplit[i];
+  }
+  if (info.b_variant[4]) {
+    const size_t zs2 = (size_t)(e->ax[0].n * (e->ax[2].n / 2) + 2 * e->ax[0].n) * sizeof(cx_t<T>);
+    AMA_CUDA_TRY(cudaFuncSetAttribute(info.b_variant[4], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zs2));
+  }
   for (int i = 0; i < 2; ++i) {
     const_cast<AmaEngine*>(e)->ac_variant[p][i][0] = info.ac_variant[i][0];
     const_cast<AmaEngine*>(e)->ac_variant[p][i][1] = info.ac_variant[i][1];
@@ -1867,16 +1888,17 @@ extern "C" int ama_engine_option(AmaEngine* e, int32_t option, int32_t value) {
       e->use_tc = value != 0;
       return AMA_OK;
     case 1:  // complex64 stage B variant: 0 shared memory, 1 register, 2 register + slot set,
-             // 3 register, two threads per column
-    case 2: {  // complex128 stage B variant (only 0 is compiled)
+             // 3 register, two threads per column, 4 shared memory split along z
+    case 2: {  // complex128 stage B variant (0 and, on long lines, 4)
       const int p = option == 1 ? AMA_C64 : AMA_C128;
       AMA_REQUIRE(e->precisions & (1u << p), AMA_ERR_ARG, "the engine was created without this precision");
-      AMA_REQUIRE(value >= 0 && value < 4, AMA_ERR_ARG, "stage B variant must be 0, 1, 2 or 3");
+      AMA_REQUIRE(value >= 0 && value < 5, AMA_ERR_ARG, "stage B variant must be 0 .. 4");
       AMA_REQUIRE(e->b_variant[p][value] != nullptr, AMA_ERR_UNSUPPORTED,
                   "this stage B variant is not compiled for the engine's grid");
       e->stage_fn[p][1] = e->b_variant[p][value];
-      e->regb[p] = value != 0;
+      e->regb[p] = value >= 1 && value <= 3;
       e->bthreads[p] = value == 3 ? 2 : 1;
+      e->zsplit[p] = e->b_zsplit[p][value];
       return AMA_OK;
     }
     case 3: {  // complex64 stages A and C: 0 shared-memory y passes, 1 y in registers (4 lanes)

@@ -76,7 +76,8 @@ struct AmaEngine {
   const void* stage_fn[2][4] = {};  // [prec][stage A, B, C, density B] (grid-specialised)
   int zsplit[2] = {1, 1};           // [prec] z halves per stage-B slab
   bool regb[2] = {false, false};    // [prec] stage B with register-resident x columns
-  const void* b_variant[2][4] = {};  // [prec] stage B variants compiled for the grid
+  const void* b_variant[2][5] = {};  // [prec] stage B variants compiled for the grid
+  int b_zsplit[2][5] = {};           // [prec] z split of each variant's shared-memory slab
   int bthreads[2] = {1, 1};          // [prec] threads per (y, z) column of the register stage B
   const void* ac_variant[2][2][2] = {};  // [prec][variant][stage A, C] compiled for the grid
   int ac_threads_of[2][2] = {};          // [prec][variant] threads per CTA of those stages

@@ -129,8 +129,8 @@ class DeviceEngine:
     def set_stage_b_variant(self, precision, variant: int) -> None:
         """Select the stage B kernel (x transforms and V): 0 shared-memory slabs, 1 register-
         resident x columns, 2 register-resident with the compile-time x-plane set, 3 register-
-        resident with two threads per column. Raises NotImplementedError when the variant is
-        not compiled for this grid."""
+        resident with two threads per column, 4 shared-memory slabs split in two along z.
+        Raises NotImplementedError when the variant is not compiled for this grid."""
         option = 1 if precision_code(precision) == AMA_C64 else 2
         call("ama_engine_option", self.handle, option, int(variant))
 

@@ -14,7 +14,9 @@ complex128 once the density residual falls below ``refine_below``, or earlier wh
 complex64 iterations stop reducing it (best of the last ``stall_window`` iterations not
 below ``stall_ratio`` times the best before them: the FP32 rounding floor of a large cell
 can sit above ``refine_below``), so the fixed point is the FP64 one. The complex64
-Davidson tolerance is floored at ``c64_tolerance_floor``; ``refine_max_iterations`` > 0 caps
+Davidson tolerance is 1e-3 of the density residual clipped to [``c64_tolerance_floor``,
+``c64_tolerance_cap``] (the reference's clip to [1e-11, 1e-6] with the FP32 noise floor and a
+looser cap while the density is far from converged); ``refine_max_iterations`` > 0 caps
 the Davidson iterations per SCF step of the FP64 refinement (the orbitals are already
 converged to the FP32 floor; the SCF convergence test itself is unchanged). Energies, densities, potentials and subspace eigensolves are FP64 always.
 """
@@ -41,6 +43,18 @@ from .potential import effective_potential, grid_ops
 from .units import EV_IN_HARTREE, HARTREE_IN_EV
 
 __all__ = ["Energies", "SCFResult", "prepare_starting_orbitals", "run_scf", "starting_orbitals"]
+
+
+def davidson_tolerance(residual: float, complex64: bool, engine) -> float:
+    """Davidson residual tolerance of an SCF step: the reference's clip(1e-3 min(residual, 1),
+    1e-11, 1e-6) (scf/driver.py:334); in the complex64 phase of the mixed policy 1e-3 of the
+    residual clipped to [c64_tolerance_floor, c64_tolerance_cap] instead: never below the FP32
+    rounding noise, and only as tight as the density residual warrants."""
+    x = 1e-3 * min(float(residual), 1.0)
+    if complex64:
+        lo = engine.c64_tolerance_floor
+        return float(np.clip(x, lo, max(engine.c64_tolerance_cap, lo)))
+    return float(np.clip(x, 1e-11, 1e-6))
 
 
 @dataclass
@@ -273,9 +287,7 @@ def run_scf(system, config: Config | None = None, *, logger=None, wavefunctions=
         H = Hamiltonian(system, veff, precision=prec_name)
         if config.engine.autotune:  # kernel variants timed once per precision on this system
             autotune_hpsi(H, nb)
-        tol = float(np.clip(1e-3 * min(residual, 1.0), 1e-11, 1e-6))
-        if orb.dtype == torch.complex64:
-            tol = max(tol, config.engine.c64_tolerance_floor)  # FP32 residuals carry rounding noise
+        tol = davidson_tolerance(residual, orb.dtype == torch.complex64, config.engine)
         maxit = 40 if iteration == 1 else 20
         if policy == "mixed" and orb.dtype == torch.complex128 and config.engine.refine_max_iterations > 0:
             maxit = config.engine.refine_max_iterations  # FP64 refinement of converged complex64 orbitals

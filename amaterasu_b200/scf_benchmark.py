@@ -10,6 +10,9 @@ residual below 1e-7 per electron:
   atomic density, the reference's start;
 * ``mixed``: complex64 bulk with tensor-core subspace products, FP64 refinement, from the
   same start;
+* ``mixed_ref_schedule``: the same with the reference's Davidson tolerance cap (1e-6) in the
+  complex64 phase instead of the policy's looser one while the density is far from
+  converged (``c64_tolerance_cap``), to show what that part of the policy contributes;
 * ``learned+mixed`` (with ``--weights``): the mixed policy from the learned start density,
   the network run on a working grid with the spacing it was trained at (0.151 A).
 
@@ -77,7 +80,8 @@ def run(workload: str, weights=None, forces=False, log=print, policies=("plain",
     prepare_starting_orbitals(system)  # the seeded start is part of the system, same for every policy
     torch.cuda.synchronize()
     setup = time.perf_counter() - t0
-    runs = [(p, {"plain": "complex128"}.get(p, "mixed"), None) for p in policies if p in ("plain", "mixed")]
+    runs = [(p, {"plain": "complex128"}.get(p, "mixed"), None) for p in policies
+            if p in ("plain", "mixed", "mixed_ref_schedule")]
     if weights and "learned+mixed" in policies:
         net = DensityNet.from_file(weights)
         cell = np.asarray(system.cell, float)
@@ -91,7 +95,10 @@ def run(workload: str, weights=None, forces=False, log=print, policies=("plain",
         torch.cuda.synchronize()
         t = time.perf_counter()
         density = start.predict(system) if start is not None else None
-        res = run_scf(system, _config(workload, precision, engine_options), density=density)
+        options = dict(engine_options or {})
+        if name == "mixed_ref_schedule":
+            options["c64_tolerance_cap"] = 1e-6
+        res = run_scf(system, _config(workload, precision, options), density=density)
         torch.cuda.synchronize()
         seconds = time.perf_counter() - t
         if hook:

@@ -62,13 +62,16 @@ def parse():
     ap.add_argument("--kpoints", type=int, default=4, help="k-points of the workload to include (profiling)")
     ap.add_argument("--no-extras", action="store_true", help="skip the e2e and complex128 legs (profiling)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the engine's default kernel variants")
-    ap.add_argument("--variants", default=None, metavar="B,AC,TC",
-                    help="force the complex64 kernel variants (stage B, stages A/C, tensor-core nonlocal 0/1) "
-                         "instead of timing them: profiling runs reproduce a timed run's choice with it")
+    ap.add_argument("--variants", default=None, metavar="B,AC,TC[,B128]",
+                    help="force the complex64 kernel variants (stage B, stages A/C, tensor-core nonlocal 0/1; "
+                         "with --config5-hpsi also the complex128 stage B) instead of timing them: profiling "
+                         "runs reproduce a timed run's choice with it")
     ap.add_argument("--no-scf", action="store_true",
                     help="skip the Si215 Gamma SCF block (plain FP64, mixed, learned+mixed; ~2 minutes)")
     ap.add_argument("--density-only", action="store_true",
                     help="time only the density accumulation (profiling)")
+    ap.add_argument("--config5-hpsi", action="store_true",
+                    help="time only the Si215 (108^3, 440 bands) H.psi in both precisions (profiling)")
     ap.add_argument("--cpu-baselines", action="store_true",
                     help="time the CPU oracle on configs 1, 3 and 5 (bounded samples; minutes) and exit")
     return ap.parse_args()
@@ -414,7 +417,7 @@ def density_leg(system, blocks, nbands, steps, stream, peak):
     return out
 
 
-def hpsi_config5(system, peak, steps=10):
+def hpsi_config5(system, peak, steps=10, variants=None):
     """H.psi of the Si215 Gamma configuration (108^3 grid, 440 bands, 80,797 plane waves)
     in both precisions on the SCF's own system: device-timed all-band calls after the
     kernel-variant autotune, with the roofline on the algorithmic bytes and the measured
@@ -435,7 +438,16 @@ def hpsi_config5(system, peak, steps=10):
         H = Hamiltonian(system, veff, precision=prec)
         psi = torch.from_numpy(block.astype(np.complex64 if prec == "complex64" else np.complex128).ravel()).cuda()
         res = torch.empty_like(psi)
-        tuned = autotune_hpsi(H, nb)
+        if variants is not None and prec == "complex64":
+            H.engine.set_stage_b_variant(prec, variants[0])
+            H.engine.set_stage_ac_variant(variants[1])
+            H.engine.set_tensor_core_nonlocal(bool(variants[2]))
+            tuned = {"stage_b": variants[0], "stage_ac": variants[1], "nonlocal_tc": bool(variants[2])}
+        elif variants is not None:
+            H.engine.set_stage_b_variant(prec, variants[3] if len(variants) > 3 else 0)
+            tuned = {"stage_b": variants[3] if len(variants) > 3 else 0}
+        else:
+            tuned = autotune_hpsi(H, nb)
         for _ in range(3):
             H.apply_all(psi, nb, out=res)
         torch.cuda.synchronize()
@@ -466,7 +478,7 @@ def scf_block(log=lambda *_: None, peak=None):
 
     after = (lambda system: hpsi_config5(system, peak)) if peak is not None else None
     out = scf_run("si215_gamma", str(weights) if weights.exists() else None, forces=True, log=log, hook=hook,
-                  after=after)
+                  after=after, policies=("plain", "mixed", "learned+mixed", "mixed_ref_schedule"))
     if "after" in out:
         out["hpsi_config5"] = out.pop("after")
     for name, row in out["runs"].items():
@@ -490,6 +502,15 @@ def main():
         return
     import torch
     import torch.distributed as dist
+
+    if args.config5_hpsi:  # profiling: the Si215 H.psi legs alone
+        from amaterasu_b200.scf_benchmark import _system
+        peaks = json.loads((REPO / "MEASURED_PEAKS.json").read_text()) if (REPO / "MEASURED_PEAKS.json").exists() else {}
+        peak = {"value": float(peaks.get("hbm_gbs", 6650.0)),
+                "source": "MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks else "fallback 6650 GB/s"}
+        variants = tuple(int(x) for x in args.variants.split(",")) if args.variants else None
+        print(json.dumps(hpsi_config5(_system("si215_gamma"), peak, steps=args.steps, variants=variants)), flush=True)
+        return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

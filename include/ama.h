@@ -71,9 +71,10 @@ AMA_API int ama_engine_destroy(AmaEngine* engine);
  *             or on the SIMT GEMM (value 0);
  *   option 1: complex64 stage B (x transforms and V) variant: 0 shared-memory slabs,
  *             1 register-resident x columns, 2 register-resident with the spheres' compile-time
- *             x-plane set, 3 register-resident with two threads per column (even x length);
+ *             x-plane set, 3 register-resident with two threads per column (even x length),
+ *             4 shared-memory slabs split in two along z (x lines of 100 or more);
  *             AMA_ERR_UNSUPPORTED when the variant is not compiled for the grid;
- *   option 2: the same for complex128 (only variant 0 exists).
+ *   option 2: the same for complex128 (variants 0 and 4).
  *   option 3: complex64 stages A and C (scatter + z, y backward; y, z forward + gather)
  *             variant: 0 shared-memory y passes, 1 y transforms in registers with four
  *             threads per column (n2 a multiple of 4 on a compile-time grid);

@@ -18,7 +18,7 @@ def _rel(a, b):
 
 def _available(eng, precision):
     out = []
-    for v in (0, 1, 2, 3):
+    for v in (0, 1, 2, 3, 4):
         try:
             eng.set_stage_b_variant(precision, v)
             out.append(v)

@@ -152,3 +152,20 @@ def test_results_round_trip_in_output_units(tmp_path, mini_system):
     np.testing.assert_allclose(out["density_internal"], dens, rtol=1e-14)
     for a, b in zip(out["wavefunctions"][0], wfs[0]):
         np.testing.assert_array_equal(a, b)
+
+
+def test_davidson_tolerance_schedule():
+    """The reference's clip(1e-3 r, 1e-11, 1e-6) in FP64; the complex64 phase floored at the
+    FP32 noise and capped at c64_tolerance_cap."""
+    from amaterasu_b200.config import EngineConfig
+    from amaterasu_b200.scf import davidson_tolerance
+    e = EngineConfig()
+    assert davidson_tolerance(0.5, False, e) == 1e-6
+    assert davidson_tolerance(1e-5, False, e) == 1e-8
+    assert davidson_tolerance(1e-12, False, e) == 1e-11
+    e.c64_tolerance_cap = 1e-6
+    assert davidson_tolerance(0.5, True, e) == e.c64_tolerance_floor  # cap below the floor
+    e.c64_tolerance_cap = 1e-4
+    assert davidson_tolerance(0.5, True, e) == 1e-4
+    assert abs(davidson_tolerance(1e-2, True, e) - 1e-5) < 1e-20
+    assert davidson_tolerance(1e-4, True, e) == e.c64_tolerance_floor

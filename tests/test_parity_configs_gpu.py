@@ -122,19 +122,21 @@ def test_si215_hpsi_matches_reference(si215_system, precision, tol):
     rng = np.random.default_rng(2150)
     psi = (rng.normal(size=(3, len(sphere))) + 1j * rng.normal(size=(3, len(sphere)))) / (1.0 + sphere.kinetic_energy)
     assert _rel(H.apply(psi, 0), g["hpsi"]) < tol
-    if precision == "complex64":  # every stage B x stage A/C variant compiled for the 108^3 grid
-        variants = []
-        for v in (0, 1, 2, 3):
-            try:
-                H.engine.set_stage_b_variant(precision, v)
-            except NotImplementedError:
-                continue
-            variants.append(v)
-            for a in (0, 1):
+    # every stage B (x stage A/C for complex64) variant compiled for the 108^3 grid
+    variants = []
+    for v in (0, 1, 2, 3, 4):
+        try:
+            H.engine.set_stage_b_variant(precision, v)
+        except NotImplementedError:
+            continue
+        variants.append(v)
+        for a in ((0, 1) if precision == "complex64" else (None,)):
+            if a is not None:
                 H.engine.set_stage_ac_variant(a)
-                assert _rel(H.apply(psi, 0), g["hpsi"]) < tol, (v, a)
-        assert variants == [0, 3]
-        H.engine.set_stage_b_variant(precision, 0)
+            assert _rel(H.apply(psi, 0), g["hpsi"]) < tol, (v, a)
+    assert variants == ([0, 3, 4] if precision == "complex64" else [0, 4])
+    H.engine.set_stage_b_variant(precision, 0)
+    if precision == "complex64":
         H.engine.set_stage_ac_variant(0)
 
 
@@ -153,6 +155,7 @@ def _first_iteration(system, precision, batched):
     c = Config()
     c.engine.batched = batched
     c.engine.precision = precision
+    c.engine.c64_tolerance_cap = 1e-6  # the reference's Davidson tolerance, not the policy's looser start
     c.occupations.scheme = "fermi-dirac"
     c.occupations.smearing = "0.01 Ha"
     c.scf.max_steps = 1
