@@ -808,12 +808,14 @@ void add_pair_variant(StageInfo& info) {
   }
 }
 
-// the shared-memory stage B with each (x, z) slab split in two along z, for long lines
-// (the whole-slab CTA of a 108^3 grid holds 93 KB (complex64) or 186 KB (complex128) of
-// shared memory, which leaves one or two CTAs per SM)
+// the shared-memory stage B with each (x, z) slab split in two along z, where the whole
+// slab is large: complex64 lines of 100 or more, complex128 lines of 40 or more (the
+// whole-slab CTA of a 108^3 grid holds 93 KB in complex64, 186 KB in complex128; of an 84^3
+// grid 113 KB in complex128, which leaves one or two CTAs per SM)
 template <typename T, int N1, int A1, int N2, int A2, int N3, int A3>
 void add_zsplit_variant(StageInfo& info) {
-  if constexpr (N3 % 2 == 0 && N1 >= 100)
+  constexpr int kMinLine = std::is_same<T, double>::value ? 40 : 100;
+  if constexpr (N3 % 2 == 0 && N1 >= kMinLine)
     info.b_variant[4] = (const void*)stage_b_kernel<T, FixDims<N1, A1, N2, A2, N3, A3, 2>>;
 }
 

@@ -72,7 +72,8 @@ AMA_API int ama_engine_destroy(AmaEngine* engine);
  *   option 1: complex64 stage B (x transforms and V) variant: 0 shared-memory slabs,
  *             1 register-resident x columns, 2 register-resident with the spheres' compile-time
  *             x-plane set, 3 register-resident with two threads per column (even x length),
- *             4 shared-memory slabs split in two along z (x lines of 100 or more);
+ *             4 shared-memory slabs split in two along z (complex64: x lines of 100 or
+ *             more; complex128: 40 or more);
  *             AMA_ERR_UNSUPPORTED when the variant is not compiled for the grid;
  *   option 2: the same for complex128 (variants 0 and 4).
  *   option 3: complex64 stages A and C (scatter + z, y backward; y, z forward + gather)

@@ -67,7 +67,8 @@ def test_every_variant_matches_the_oracle(mini_system, precision, tol):
 
 def test_si64_variants_match_the_reference(si_pseudo):
     """84^3 grid: shared-memory, register, sparse register and two-lane register stage B
-    against the golden."""
+    (complex64), whole-slab and z-split shared-memory stage B (complex128), against the
+    golden."""
     from amaterasu_b200.autotune import autotune_hpsi
     from amaterasu_b200.cells import workload
     from amaterasu_b200.hamiltonian import Hamiltonian
@@ -95,12 +96,24 @@ def test_si64_variants_match_the_reference(si_pseudo):
     choice = autotune_hpsi(H, 32)
     print("autotune", choice)
     assert choice["stage_b"] in variants and choice["stage_ac"] in ac
+    # complex128: the whole-slab and the z-split shared-memory stage B
+    H2 = Hamiltonian(s, veff.cpu().numpy(), precision="complex128")
+    v128 = _available(H2.engine, "complex128")
+    assert v128 == [0, 4]
+    for v in v128:
+        H2.engine.set_stage_b_variant("complex128", v)
+        for ik, nbk in ((0, 2), (1, 1)):
+            w = s.wave_spheres[ik]
+            rng = np.random.default_rng(300 + ik)
+            psi = (rng.normal(size=(nbk, len(w))) + 1j * rng.normal(size=(nbk, len(w)))) / (1.0 + w.kinetic_energy)
+            assert _rel(H2.apply(psi, ik), g[f"hpsi{ik}"]) < 1e-11, (v, ik)
+    H2.engine.set_stage_b_variant("complex128", 0)
     torch.cuda.synchronize()
 
 
 def test_si8_grid_variants_match_the_oracle(si_pseudo):
-    """42^3 grid (the 260-k Si8 configuration's): every stage B variant, on two k-points of
-    its mesh with 20 bands, against the oracle's FP64 H.psi."""
+    """42^3 grid (the 260-k Si8 configuration's): every stage B variant of both precisions,
+    on two k-points of its mesh with 20 bands, against the oracle's FP64 H.psi."""
     from amaterasu_b200 import kpoints as kp
     from amaterasu_b200.cells import workload
     from amaterasu_b200.hamiltonian import Hamiltonian
@@ -122,3 +135,13 @@ def test_si8_grid_variants_match_the_oracle(si_pseudo):
             ref = hamiltonian_apply(psi, w.miller, s.grid.shape, w.kinetic_energy, veff[0],
                                     s.projectors[ik].matrix, s.projectors[ik].dij)
             assert _rel(H.apply(psi, ik), ref) < 2e-5, (v, ik)
+    H2 = Hamiltonian(s, veff, precision="complex128")
+    assert _available(H2.engine, "complex128") == [0, 4]
+    for v in (0, 4):
+        H2.engine.set_stage_b_variant("complex128", v)
+        for ik, w in enumerate(s.wave_spheres):
+            psi = (rng.normal(size=(nb, len(w))) + 1j * rng.normal(size=(nb, len(w)))) / (1.0 + w.kinetic_energy)
+            ref = hamiltonian_apply(psi, w.miller, s.grid.shape, w.kinetic_energy, veff[0],
+                                    s.projectors[ik].matrix, s.projectors[ik].dij)
+            assert _rel(H2.apply(psi, ik), ref) < 1e-11, (v, ik)
+    H2.engine.set_stage_b_variant("complex128", 0)
