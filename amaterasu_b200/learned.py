@@ -272,12 +272,21 @@ class LearnedStart:
         n0 = system.initial_density()  # (nspin, ...)
         total0 = n0.sum(axis=0)
         try:
-            work = fourier_resample(total0, (self.grid,) * 3)
+            same = tuple(system.grid.shape) == (self.grid,) * 3
+            if same:  # the resampling is a band limit: one grid-filter pass on the device
+                from .potential import grid_ops
+                ops = grid_ops(system)
+                work = ops.band_limit(torch.from_numpy(total0)).reshape(total0.shape).cpu().numpy()
+            else:
+                work = fourier_resample(total0, (self.grid,) * 3)
             strain = strain_of(system.cell, self.reference_cell)
             x = torch.from_numpy(network_input(np.maximum(work, 1e-12), strain)[None]).to(self.net.device)
             delta, _ = self.net.forward(x)
-            delta = np.clip(delta[0, 0].cpu().numpy().astype(float), -5.0, 5.0)
-            log_corr = fourier_resample(delta, tuple(system.grid.shape))
+            delta = torch.clamp(delta[0, 0].to(torch.float64), -5.0, 5.0)
+            if same:
+                log_corr = ops.band_limit(delta).reshape(total0.shape).cpu().numpy()
+            else:
+                log_corr = fourier_resample(delta.cpu().numpy(), tuple(system.grid.shape))
             pred = finalize(total0 * np.exp(log_corr), system.nelectrons, system.grid.cell_volume_per_point)
             if not np.all(np.isfinite(pred)):
                 raise FloatingPointError("non-finite prediction")

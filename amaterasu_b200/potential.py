@@ -19,6 +19,7 @@ from .engine import engine_for, ptr, stream_ptr
 
 HARTREE_SLOT = 0
 KERKER_SLOT = 1
+BANDLIMIT_SLOT = 2
 #: functional name (as the reference spells it, case-insensitive) -> (kind, GGA code)
 FUNCTIONALS = {"LDA-PZ": ("lda", None), "PBE": ("gga", 0), "PBESOL": ("gga", 1)}
 
@@ -82,6 +83,25 @@ class GridOps:
         out = torch.empty_like(field)
         call("ama_grid_filter", self.engine.handle, KERKER_SLOT, -1, ptr(field), ptr(out), None,
              stream_ptr())
+        return out
+
+    def band_limit(self, field: torch.Tensor) -> torch.Tensor:
+        """The field with every Fourier component at or beyond the Nyquist frequency of an
+        even axis removed (|m_a| <= (n_a - 1) // 2 kept): the same-shape case of a
+        band-limited resampling, as one grid-filter pass on the device."""
+        if not getattr(self, "_band_limit_set", False):
+            keep = np.ones(self.shape)
+            for a, n in enumerate(self.shape):
+                if n % 2 == 0:
+                    idx = [slice(None)] * 3
+                    idx[a] = n // 2
+                    keep[tuple(idx)] = 0.0
+            call("ama_set_grid_filter", self.engine.handle, BANDLIMIT_SLOT,
+                 np.ascontiguousarray(keep.ravel()).ctypes.data_as(ct.c_void_p))
+            self._band_limit_set = True
+        field = field.reshape(-1).to(self.device, torch.float64).contiguous()
+        out = torch.empty_like(field)
+        call("ama_grid_filter", self.engine.handle, BANDLIMIT_SLOT, -1, ptr(field), ptr(out), None, stream_ptr())
         return out
 
     def lda(self, density: torch.Tensor):

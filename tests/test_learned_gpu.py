@@ -110,3 +110,19 @@ def test_learned_start_is_a_valid_density(mini_system):
     assert d.shape == (1, *s.grid.shape)
     assert np.all(d > 0)
     np.testing.assert_allclose(d.sum() * s.grid.cell_volume_per_point, s.nelectrons, rtol=1e-12)
+
+
+def test_band_limit_matches_fourier_resample(mini_system):
+    """The device band limit (one grid-filter pass) equals the host same-shape Fourier
+    resampling the learned start used to run (Nyquist planes of even axes removed), to
+    1e-12 of the field's scale."""
+    import torch
+    from amaterasu_b200.learned import fourier_resample
+    from amaterasu_b200.potential import grid_ops
+    s = mini_system
+    assert all(n % 2 == 0 for n in s.grid.shape)
+    rng = np.random.default_rng(11)
+    f = s.initial_density()[0] * np.exp(0.3 * rng.normal(size=s.grid.shape))
+    ref = fourier_resample(f, tuple(s.grid.shape))
+    got = grid_ops(s).band_limit(torch.from_numpy(f)).reshape(s.grid.shape).cpu().numpy()
+    assert np.abs(got - ref).max() < 1e-12 * np.abs(ref).max()
