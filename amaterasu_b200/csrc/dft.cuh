@@ -339,6 +339,24 @@ __device__ void contig_rows(C* sm, int n, int ld, const int* rows, int nrows, co
   }
 }
 
+// The contiguous column pass writing its output to a global array with the same
+// (n x ncols) layout instead of back to shared memory: the last pass of a natural-in
+// transform stores straight to HBM, and the plane copy from shared memory disappears.
+template <int RB, int S, int NT = kFftThreads, typename C>
+__device__ void contig_cols_to(const C* sm, C* __restrict__ g, int n, int ncols) {
+  const int A = n / RB;
+  const int tasks = A * ncols;
+  for (int t = threadIdx.x; t < tasks; t += NT) {
+    const int col = t % ncols, c = t / ncols;
+    C v[RB];
+#pragma unroll
+    for (int d = 0; d < RB; ++d) v[d] = sm[(c * RB + d) * ncols + col];
+    dft_reg<RB, S>(v);
+#pragma unroll
+    for (int d = 0; d < RB; ++d) g[(int64_t)(c * RB + d) * ncols + col] = v[d];
+  }
+}
+
 // Supported codelet lengths (1..16 except 13); dispatch a runtime length to a template.
 #define AMA_RADIX_CASES(X) \
   X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(14) X(15) X(16)
@@ -376,6 +394,23 @@ __device__ void dft_cols(C* sm, int n, int A, int B, int ncols, const C* tw) {
 #undef CASE
     }
     __syncthreads();
+  }
+}
+
+// dft_cols (natural in, permuted out) with the contiguous pass writing to the global
+// plane `g` (same layout) instead of back to shared memory.
+template <int S, int NT = kFftThreads, typename C>
+__device__ void dft_cols_store(C* sm, C* __restrict__ g, int n, int A, int B, int ncols, const C* tw) {
+  switch (A) {
+#define CASE(R) case R: strided_cols<R, S, true, NT>(sm, n, ncols, tw); break;
+    AMA_RADIX_CASES(CASE)
+#undef CASE
+  }
+  __syncthreads();
+  switch (B) {
+#define CASE(R) case R: contig_cols_to<R, S, NT>(sm, g, n, ncols); break;
+    AMA_RADIX_CASES(CASE)
+#undef CASE
   }
 }
 
