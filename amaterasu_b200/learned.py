@@ -4,7 +4,7 @@ The network maps the superposed atomic density n0 (the reference's start density
 amaterasu ``hamiltonian/local.py:77-106``) and the cell strain to a correction
 Delta(r); the start density is n0 exp(Delta), renormalised to the electron count and
 floored at zero exactly like the superposition (``local.py:102-105``), so a poor prediction
-can only cost SCF iterations, never move the fixed point: the converged SCF is the judge.
+can only cost SCF iterations, never move the fixed point: the converged SCF decides.
 
 Architecture (36^3 working grid, circular padding, 3x3x3 kernels, SiLU):
   enc1  8 -> 16 -> 16            (36^3)
