@@ -6,12 +6,13 @@ x-plane set fixed at compile time, for the benchmark grid; register-resident wit
 threads per column, for even x lengths up to 108; shared-memory slabs split in two along z,
 for the long lines of a 108^3 grid), two variants of the stages around it
 (y transforms in shared memory or in registers with four lanes per column) and two paths
-for the complex64 nonlocal products (tcgen05 split-TF32 GEMMs or SIMT GEMMs). Which is fastest depends on the
-grid, the band count and the number of k-points of a call. ``autotune_hpsi`` times every
-available combination on the caller's Hamiltonian and block shape (CUDA events on the
-current stream after one warm-up call each), leaves the engine set to the fastest and
-returns the measurements; results are cached per (precision, nbands, k-point range) on the
-engine. All variants compute the same H.psi (``tests/test_autotune_gpu.py``).
+for the complex64 nonlocal products (tcgen05 split-TF32 GEMMs or SIMT GEMMs). Which is
+fastest depends on the grid, the band count and the number of k-points of a call.
+``autotune_hpsi`` times every stage combination on the caller's Hamiltonian and block shape
+(CUDA events on the current stream after one warm-up call each), and the SIMT nonlocal
+alternative only with the fastest stage pair, the two parts' times being additive; it
+leaves the engine set to the fastest and returns the measurements. Results are cached per
+(precision, nbands, k-point range) on the engine. All variants compute the same H.psi (``tests/test_autotune_gpu.py``).
 """
 from __future__ import annotations
 
@@ -69,24 +70,32 @@ def autotune_hpsi(H, nbands: int, *, k_first: int = 0, k_count: int | None = Non
     g = torch.Generator(device=eng.device).manual_seed(7)
     psi = torch.randn(n, dtype=TORCH_DTYPE[prec], device=eng.device, generator=g)
     out = torch.empty_like(psi)
-    paths = [True, False] if (prec == 0 and eng.nproj > 0) else [True]
     times = {}
     stream = torch.cuda.current_stream(eng.device)
-    for v in _variants(eng, prec):
+
+    def time_call(v, a, tc):
         eng.set_stage_b_variant(prec, v)
+        if prec == 0:
+            eng.set_stage_ac_variant(a)
+        eng.set_tensor_core_nonlocal(tc)
+        H.apply_all(psi, nbands, k_first=k_first, k_count=k_count, out=out)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            H.apply_all(psi, nbands, k_first=k_first, k_count=k_count, out=out)
+        e1.record(stream)
+        torch.cuda.synchronize(eng.device)
+        times[(v, a, tc)] = e0.elapsed_time(e1) / reps
+
+    # The FFT stages and the nonlocal products are separate launches in stream order, so
+    # their times add: time every stage pair with the tensor-core products, then the SIMT
+    # products only with the fastest stage pair.
+    for v in _variants(eng, prec):
         for a in _ac_variants(eng, prec):
-            if prec == 0:
-                eng.set_stage_ac_variant(a)
-            for tc in paths:
-                eng.set_tensor_core_nonlocal(tc)
-                H.apply_all(psi, nbands, k_first=k_first, k_count=k_count, out=out)
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-                for _ in range(reps):
-                    H.apply_all(psi, nbands, k_first=k_first, k_count=k_count, out=out)
-                e1.record(stream)
-                torch.cuda.synchronize(eng.device)
-                times[(v, a, tc)] = e0.elapsed_time(e1) / reps
+            time_call(v, a, True)
+    if prec == 0 and eng.nproj > 0:
+        v, a, _ = min(times, key=times.get)
+        time_call(v, a, False)
     best = min(times, key=times.get)
     eng.set_stage_b_variant(prec, best[0])
     if prec == 0:
