@@ -57,6 +57,7 @@ SIGNATURES = {
     "ama_grid_divergence": (ct.c_int, [_P, _P, _P, ct.c_double, ct.c_double, _P, _P]),
     "ama_xc_gga": (ct.c_int, [_P, _I32, _I32, _P, _P, _P, _P, _P]),
     "ama_davidson": (ct.c_int, [_P, _I32, _I32, _I32, _P, _D, _I32, _I32, _P, _P, _P, _P, _P]),
+    "ama_davidson_graph_stats": (ct.c_int, [ct.POINTER(_I64), ct.POINTER(_I64), ct.POINTER(_I64), _I32]),
     "ama_engine_option": (ct.c_int, [_P, _I32, _I32]),
     "ama_tc_status": (ct.c_int, [_P, ct.POINTER(ct.c_int32)]),
     "ama_set_potential": (ct.c_int, [_P, _P, _I32, _P]),

@@ -45,9 +45,17 @@ class _KOp:
                              int(ld), int(kstride))
 
 
+def graph_stats(reset: bool = False) -> dict:
+    """ama_davidson's iteration segments on this thread and the current device: captured as
+    CUDA graphs, replayed from a graph, launched kernel by kernel."""
+    c, r, n = ct.c_int64(0), ct.c_int64(0), ct.c_int64(0)
+    call("ama_davidson_graph_stats", ct.byref(c), ct.byref(r), ct.byref(n), 1 if reset else 0)
+    return {"captured": int(c.value), "replayed": int(r.value), "launched": int(n.value)}
+
+
 class BatchedDavidson:
     def __init__(self, system, nbands: int, dtype=torch.complex128, tensor_cores: bool = True,
-                 tc_min_npw: int = _TC_MIN_NPW):
+                 tc_min_npw: int = _TC_MIN_NPW, graphs: bool = True):
         self.eng = engine_for(system)
         self.system = system
         self.nk = self.eng.nk
@@ -67,6 +75,7 @@ class BatchedDavidson:
         # long enough for the staged tiles to pay; shorter ones stay on the SIMT kernels
         self.tensor_cores = bool(tensor_cores) and dtype == torch.complex64 and self.max_npw >= tc_min_npw
         self.tc_min_npw = int(tc_min_npw)
+        self.graphs = bool(graphs)  # ama_davidson replays recurring iteration segments as CUDA graphs
         self.trace = []  # per iteration of the last run: (iteration, active directions, subspace size, max norm)
 
     # ---------------------------------------------------------------- kernels
@@ -214,6 +223,7 @@ class BatchedDavidson:
         X = torch.empty_like(guess)
         it = ct.c_int32(0)
         tc_min = self.tc_min_npw if self.tensor_cores else 0
+        self.eng.set_davidson_graphs(self.graphs)
         call("ama_davidson", self.eng.handle, self.prec, int(spin), self.nb, ptr(guess), float(tolerance),
              int(max_iterations), int(tc_min), ptr(eps), ptr(X), ptr(norms), ct.byref(it), stream_ptr())
         return eps.cpu().numpy(), X, norms.cpu().numpy(), int(it.value)

@@ -81,6 +81,8 @@ class EngineConfig:
     # the SCF convergence test is unchanged
     refine_max_iterations: int = 4
     batched: bool = True
+    # the batched Davidson replays its recurring iteration segments as CUDA graphs
+    davidson_graphs: bool = True
 
 
 @dataclass

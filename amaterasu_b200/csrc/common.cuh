@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <string>
+#include <atomic>
 #include <utility>
 #include <type_traits>
 
@@ -42,6 +43,13 @@ template <int N, class F> __device__ __forceinline__ void static_for(F&& f) {
 
 // Thread-local last-error message for the C-ABI.
 void set_error(const std::string& msg);
+
+// Generation of the library's allocations. Every allocation, growth or free of device or
+// pinned memory that a kernel or copy may reference (scratch, engine tables, engine option
+// changes that swap kernels) bumps it; a cached CUDA graph holds raw pointers and launch
+// shapes, so it is replayed only while the generation it was captured in is current.
+uint64_t memory_epoch();
+void bump_memory_epoch();
 
 // Library state that holds device memory is kept per CUDA device: a process that drives
 // several GPUs must never hand one device's buffer to a kernel on another.

@@ -9,11 +9,21 @@
 // not fit under 4 nbands. Batched over k, every step is one launch over all k-points (ragged
 // plane-wave counts). A k-point with fewer new directions than the others carries zero
 // rows marked invalid; their Rayleigh-Ritz diagonal is set just above that k-point's
-// Gershgorin bound, which decouples them without inflating the matrix norm. The host
-// synchronises three times per iteration for all k-points together: the residual norms (which
-// bands are active), the rank test of the new directions, and the admissibility of the
-// Newton-Schulz orthonormalisation (the new directions' overlap within 0.5 of the identity
-// in Frobenius norm; otherwise their overlap is decomposed).
+// Gershgorin bound, which decouples them without inflating the matrix norm.
+//
+// The host synchronises twice per iteration for all k-points together, and every shape
+// decision is made there: (1) after the residual norms (how many bands are active: the
+// block width nn), (2) after the rank test of the new directions and their overlap's
+// distance from the identity (whether any direction survived; whether the Newton-Schulz
+// orthonormalisation is admissible, the overlap within 0.5 of the identity in Frobenius
+// norm, and how many of its steps are needed; otherwise the overlap is decomposed). Which
+// bands are active, which rows are valid and the eigenvalues stay on the device. The work
+// between two synchronisations is a segment whose launches depend only on (basis size,
+// block width, Newton-Schulz steps); a segment seen before is captured once as a CUDA graph
+// and replayed from then on (every buffer it touches is owned by the library and the
+// library's allocation generation tells when a pointer in a graph went stale). Segments
+// whose eigensolves are above the batched Jacobi order run launch by launch: their kernels
+// are long and the tridiagonal reduction is a cooperative launch.
 //
 // Orthonormalisation: the rank-revealing pass uses the overlap's eigendecomposition (which
 // spans the same space as the reference's SVD); the second pass (the reference's Cholesky)
@@ -23,6 +33,7 @@
 #include "engine_impl.cuh"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <vector>
 
@@ -33,6 +44,7 @@ namespace {
 constexpr int kSmT = 256;
 constexpr int kJacobiMax = 80;
 constexpr double kGap = 1.0;  // Ha above the Gershgorin bound for invalid rows
+constexpr int kGraphCacheMax = 48;  // executable graphs kept per device and host thread
 
 // out[k][i][j] = v_i v_j (a'_ij + conj(a'_ji)) / 2 + (1 - v_i) delta_ij inval_diag,
 // a' = conj(a) when conj_in, a the k-th (n x n) block (row-major, leading dimension n) of
@@ -190,29 +202,80 @@ __global__ void __launch_bounds__(kSmT) to_precision_kernel(const double2* __res
     out[q] = mk<cx_t<T>>(in[q].x, in[q].y);
 }
 
+// rows[k][b] = rank of band b among k's bands whose residual norm is above *tol, or -1
+// (converged); one thread per k-point, bands in order.
+__global__ void __launch_bounds__(kSmT) active_rows_kernel(const double* __restrict__ nrm, const double* __restrict__ tol,
+                                                           int nk, int nb, int32_t* __restrict__ rows) {
+  const int k = blockIdx.x * kSmT + threadIdx.x;
+  if (k >= nk) return;
+  const double t = *tol;
+  int c = 0;
+  for (int b = 0; b < nb; ++b) rows[(int64_t)k * nb + b] = nrm[(int64_t)k * nb + b] > t ? c++ : -1;
+}
+
+// valid[k][i] = (i < count) for i < cap: the basis holds `count` valid rows per k-point.
+__global__ void __launch_bounds__(kSmT) valid_prefix_kernel(uint8_t* __restrict__ valid, int nk, int cap, int count) {
+  for (int64_t t = blockIdx.x * (int64_t)kSmT + threadIdx.x; t < (int64_t)nk * cap; t += (int64_t)gridDim.x * kSmT)
+    valid[t] = (t % cap) < count;
+}
+
+// valid[k][m + i] = keep[k][i] for i < nn: the rank test's verdict on the appended rows.
+__global__ void __launch_bounds__(kSmT) valid_append_kernel(uint8_t* __restrict__ valid, const uint8_t* __restrict__ keep,
+                                                            int nk, int cap, int m, int nn) {
+  for (int64_t t = blockIdx.x * (int64_t)kSmT + threadIdx.x; t < (int64_t)nk * nn; t += (int64_t)gridDim.x * kSmT) {
+    const int64_t k = t / nn, i = t - k * nn;
+    valid[k * cap + m + i] = keep[t];
+  }
+}
+
 int blocks_for(int64_t count) { return (int)std::max<int64_t>(1, std::min<int64_t>((count + kSmT - 1) / kSmT, 4 * 148)); }
 
-// A device buffer that only grows.
-struct Buf {
+// A device (or pinned host) buffer that only grows.
+template <bool Host>
+struct GrowBuf {
   void* p = nullptr;
   size_t bytes = 0;
   int need(size_t b) {
     if (bytes >= b) return AMA_OK;
-    if (p) AMA_CUDA_TRY(cudaFree(p));
+    bump_memory_epoch();
+    if (p) AMA_CUDA_TRY(Host ? cudaFreeHost(p) : cudaFree(p));
     p = nullptr;
     bytes = 0;
-    AMA_CUDA_TRY(cudaMalloc(&p, std::max<size_t>(b, 256)));
-    bytes = std::max<size_t>(b, 256);
+    const size_t sz = std::max<size_t>(b, 256);
+    AMA_CUDA_TRY(Host ? cudaMallocHost(&p, sz) : cudaMalloc(&p, sz));
+    bytes = sz;
     return AMA_OK;
   }
   template <typename X> X* as() const { return static_cast<X*>(p); }
+};
+using Buf = GrowBuf<false>;
+using HostBuf = GrowBuf<true>;
+
+// Executable graphs of iteration segments, keyed by everything their launches depend on.
+using SegKey = std::array<int64_t, 10>;
+struct GraphCache {
+  uint64_t epoch = 0;
+  std::vector<std::pair<SegKey, cudaGraphExec_t>> execs;
+  std::vector<SegKey> seen, refused;
+  int64_t captured = 0, replayed = 0, launched = 0;
+  // only called with the segment stream idle (right after a host synchronisation)
+  void drop() {
+    for (auto& x : execs) cudaGraphExecDestroy(x.second);
+    execs.clear();
+    seen.clear();
+    refused.clear();
+  }
 };
 
 struct DavWork {
   Buf B, HB, X, HX, O1, O2, C, HN, X0;          // packed per-k blocks
   Buf p, t, rot;                                // small, working precision
   Buf g, y, z, tt, tmp;                         // small, FP64 complex
-  Buf w, dev, keep, valid, rows, nrm;           // per-k vectors
+  Buf w, dev, keep, valid, rows, nrm, eps, tol; // per-k vectors
+  HostBuf h_norms, h_keep, h_dev, h_tol;        // pinned: what the host decides on
+  cudaStream_t stream = nullptr;                // the library's own (capturable) stream
+  cudaEvent_t ready = nullptr;
+  GraphCache graphs;
 };
 thread_local PerDevice<DavWork> g_dav;
 
@@ -222,19 +285,78 @@ struct Davidson {
   AmaEngine* e;
   int prec, spin, nb, nk, cap, max_sub, max_npw;
   int64_t total_pw;
-  bool tc;
+  bool tc, graphs;
   cudaStream_t s;
   DavWork& wk;
-  std::vector<uint8_t> valid;  // [nk][cap]
 
-  Davidson(AmaEngine* e_, int prec_, int spin_, int nb_, bool tc_, cudaStream_t s_, DavWork& wk_)
-      : e(e_), prec(prec_), spin(spin_), nb(nb_), nk(e_->nk), tc(tc_), s(s_), wk(wk_) {
+  Davidson(AmaEngine* e_, int prec_, int spin_, int nb_, bool tc_, bool graphs_, cudaStream_t s_, DavWork& wk_)
+      : e(e_), prec(prec_), spin(spin_), nb(nb_), nk(e_->nk), tc(tc_), graphs(graphs_), s(s_), wk(wk_) {
     max_npw = e->max_npw;
     total_pw = e->pw_off[nk];
     int min_npw = *std::min_element(e->npw.begin(), e->npw.end());
     max_sub = std::min(4 * nb, min_npw);
     cap = max_sub + nb;
-    valid.assign((size_t)nk * cap, 0);
+  }
+
+  SegKey key(int seg, int m, int nn, int ns_steps, int tail) const {
+    return {(int64_t)(intptr_t)e, prec, spin, nb, nk, tc ? 1 : 0, seg, m, nn, (int64_t)ns_steps * 2 + tail};
+  }
+
+  // Runs `body` (launches on s only, no host synchronisation, no host state changed) as a
+  // CUDA graph when this segment was seen before in the current allocation generation:
+  // the first occurrence launches directly (and grows every buffer the segment needs), the
+  // second is captured, later ones replay. A capture that fails (or that saw an allocation)
+  // is discarded and the segment is launched directly instead, then and from then on.
+  template <class F>
+  int segment(const SegKey& k, bool capturable, F&& body) {
+    GraphCache& gc = wk.graphs;
+    if (!graphs || !capturable) {
+      ++gc.launched;
+      return body();
+    }
+    const uint64_t ep = memory_epoch();
+    if (gc.epoch != ep) {
+      gc.drop();
+      gc.epoch = ep;
+    }
+    for (auto& x : gc.execs)
+      if (x.first == k) {
+        AMA_CUDA_TRY(cudaGraphLaunch(x.second, s));
+        ++gc.replayed;
+        return AMA_OK;
+      }
+    auto has = [&k](const std::vector<SegKey>& v) { return std::find(v.begin(), v.end(), k) != v.end(); };
+    if (!has(gc.seen) || has(gc.refused)) {
+      if (gc.seen.size() > 1024) gc.seen.clear();
+      if (!has(gc.seen)) gc.seen.push_back(k);
+      ++gc.launched;
+      return body();
+    }
+    if ((int)gc.execs.size() >= kGraphCacheMax) {
+      cudaGraphExecDestroy(gc.execs.front().second);
+      gc.execs.erase(gc.execs.begin());
+    }
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    bool good = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (good) {
+      const int rc = body();
+      const cudaError_t ce = cudaStreamEndCapture(s, &graph);
+      good = rc == AMA_OK && ce == cudaSuccess && graph != nullptr && memory_epoch() == ep &&
+             cudaGraphInstantiate(&exec, graph, 0ULL) == cudaSuccess;
+      if (graph) cudaGraphDestroy(graph);
+    }
+    if (!good) {
+      (void)cudaGetLastError();
+      if (exec) cudaGraphExecDestroy(exec);
+      gc.refused.push_back(k);
+      ++gc.launched;
+      return body();
+    }
+    gc.execs.emplace_back(k, exec);
+    ++gc.captured;
+    AMA_CUDA_TRY(cudaGraphLaunch(exec, s));
+    return AMA_OK;
   }
 
   size_t esz() const { return sizeof(C); }
@@ -288,8 +410,9 @@ struct Davidson {
 
   int apply(const void* blk, int rows, void* out) { return ama_hpsi(e, prec, 0, nk, rows, spin, blk, out, s); }
 
-  // Orthonormal rows spanning the dominant part of each k's block -> out; keep [nk][rows] on the host
-  int orthonormal_rows(void* blk, int rows, double threshold, bool drop_small, void* out, std::vector<uint8_t>& keep) {
+  // Orthonormal rows spanning the dominant part of each k's block -> out; which of them are
+  // kept -> wk.keep [nk][rows] (device)
+  int orthonormal_rows(void* blk, int rows, double threshold, bool drop_small, void* out) {
     if (int rc = gram(blk, rows, nullptr, 0, 0.0)) return rc;
     double2* g = wk.g.as<double2>();
     if (drop_small) {
@@ -302,35 +425,39 @@ struct Davidson {
     inv_sqrt_rotation_kernel<T><<<nk, kSmT, 0, s>>>(g, wk.w.as<double>(), wk.rot.as<C>(), wk.keep.as<uint8_t>(), rows,
                                                     threshold);
     AMA_CHECK_LAUNCH();
-    if (int rc = rotate(wk.rot.p, blk, rows, rows, rows, out)) return rc;
-    keep.resize((size_t)nk * rows);
-    AMA_CUDA_TRY(cudaMemcpyAsync(keep.data(), wk.keep.p, keep.size(), cudaMemcpyDeviceToHost, s));
-    AMA_CUDA_TRY(cudaStreamSynchronize(s));
+    return rotate(wk.rot.p, blk, rows, rows, rows, out);
+  }
+
+  // The FP64 overlap of the rows of blk that wk.keep marks (others set to the identity) ->
+  // wk.g, and its Frobenius distance from the identity -> wk.dev [nk] (device).
+  int lowdin_measure(void* blk, int rows) {
+    if (int rc = gram(blk, rows, wk.keep.as<uint8_t>(), rows, 1.0)) return rc;
+    frobenius_deviation_kernel<<<nk, kSmT, 0, s>>>(wk.g.as<double2>(), rows, wk.dev.as<double>());
+    AMA_CHECK_LAUNCH();
     return AMA_OK;
   }
 
-  // Newton-Schulz (coupled Y <- Y T, Z <- T Z, T = (3I - Z Y)/2) for S^{-1/2} of rows that are
-  // orthonormal to rounding; *ok = false when the overlap is too far from the identity.
-  int lowdin_rows(void* blk, int rows, const std::vector<uint8_t>& keep, void* out, bool* ok) {
-    *ok = false;
-    if (int rc = wk.valid.need((size_t)nk * rows)) return rc;
-    AMA_CUDA_TRY(cudaMemcpyAsync(wk.valid.p, keep.data(), (size_t)nk * rows, cudaMemcpyHostToDevice, s));
-    if (int rc = gram(blk, rows, wk.valid.as<uint8_t>(), rows, 1.0)) return rc;
-    if (int rc = wk.dev.need((size_t)nk * sizeof(double))) return rc;
-    frobenius_deviation_kernel<<<nk, kSmT, 0, s>>>(wk.g.as<double2>(), rows, wk.dev.as<double>());
-    AMA_CHECK_LAUNCH();
-    std::vector<double> dev(nk);
-    AMA_CUDA_TRY(cudaMemcpyAsync(dev.data(), wk.dev.p, nk * sizeof(double), cudaMemcpyDeviceToHost, s));
-    AMA_CUDA_TRY(cudaStreamSynchronize(s));
+  // Newton-Schulz steps for the measured distance (host copy in wk.h_dev), or -1 when the
+  // overlap is too far from the identity: every step squares the error, stop at 1e-18.
+  int newton_schulz_steps() const {
     double dmax = 0.0;
-    for (double d : dev) dmax = std::isnan(d) ? INFINITY : std::max(dmax, d);
-    if (!(dmax < 0.5)) return AMA_OK;
+    for (int k = 0; k < nk; ++k) {
+      const double d = wk.h_dev.as<double>()[k];
+      dmax = std::isnan(d) ? INFINITY : std::max(dmax, d);
+    }
+    if (!(dmax < 0.5)) return -1;
     int iters = 0;
     double err = std::max(dmax, 1e-300);
     while (err > 1e-18 && iters < 6) {
       err *= err;
       ++iters;
     }
+    return iters;
+  }
+
+  // Newton-Schulz (coupled Y <- Y T, Z <- T Z, T = (3I - Z Y)/2) for S^{-1/2} of the overlap
+  // in wk.g (rows orthonormal to rounding), applied to blk -> out.
+  int lowdin_apply(void* blk, int rows, int iters, void* out) {
     const size_t sb = (size_t)nk * rows * rows * sizeof(double2);
     if (int rc = wk.y.need(sb)) return rc;
     if (int rc = wk.z.need(sb)) return rc;
@@ -358,20 +485,17 @@ struct Davidson {
     if (int rc = wk.rot.need((size_t)nk * rows * rows * esz())) return rc;
     to_precision_kernel<T><<<nb_, kSmT, 0, s>>>(z, wk.rot.as<C>(), (int64_t)nk * rows * rows);
     AMA_CHECK_LAUNCH();
-    if (int rc = rotate(wk.rot.p, blk, rows, rows, rows, out)) return rc;
-    *ok = true;
-    return AMA_OK;
+    return rotate(wk.rot.p, blk, rows, rows, rows, out);
   }
 
-  // Rayleigh-Ritz over the first m rows of B / HB: eigenvalues -> eps [nk][nb], X, HX
-  int rayleigh_ritz(int m, double* eps) {
+  // Rayleigh-Ritz over the first m rows of B / HB (validity wk.valid): eigenvalues -> wk.eps
+  // [nk][nb], Ritz vectors -> X, HX
+  int rayleigh_ritz(int m) {
     if (int rc = wk.p.need((size_t)nk * m * m * esz())) return rc;
     if (int rc = wk.g.need((size_t)nk * m * m * sizeof(double2))) return rc;
     if (int rc = gemm(1, m, m, -1, op(wk.B.p, cap, 0, 1), op(wk.HB.p, cap, 0, 1),
                       op(wk.p.p, 0, 0, 0, m, (int64_t)m * m)))
       return rc;
-    if (int rc = wk.valid.need((size_t)nk * cap)) return rc;
-    AMA_CUDA_TRY(cudaMemcpyAsync(wk.valid.p, valid.data(), valid.size(), cudaMemcpyHostToDevice, s));
     double2* g = wk.g.as<double2>();
     small_hermitise_kernel<T><<<blocks_for((int64_t)nk * m * m), kSmT, 0, s>>>(wk.p.as<C>(), g, nk, m, 1,
                                                                               wk.valid.as<uint8_t>(), cap, 0.0);
@@ -384,101 +508,147 @@ struct Davidson {
     AMA_CHECK_LAUNCH();
     if (int rc = rotate(wk.rot.p, wk.B.p, cap, m, nb, wk.X.p)) return rc;
     if (int rc = rotate(wk.rot.p, wk.HB.p, cap, m, nb, wk.HX.p)) return rc;
-    AMA_CUDA_TRY(cudaMemcpy2DAsync(eps, nb * sizeof(double), wk.w.p, m * sizeof(double), nb * sizeof(double), nk,
-                                   cudaMemcpyDeviceToDevice, s));
+    AMA_CUDA_TRY(cudaMemcpy2DAsync(wk.eps.p, nb * sizeof(double), wk.w.p, m * sizeof(double), nb * sizeof(double),
+                                   nk, cudaMemcpyDeviceToDevice, s));
     return AMA_OK;
   }
 
-  int run(const void* guess, double tol, int maxit, double* eps, void* x_out, double* norms_out, int* iterations) {
+  int valid_prefix(int count) {
+    valid_prefix_kernel<<<blocks_for((int64_t)nk * cap), kSmT, 0, s>>>(wk.valid.as<uint8_t>(), nk, cap, count);
+    AMA_CHECK_LAUNCH();
+    return AMA_OK;
+  }
+
+  // residual norms of the Ritz pairs -> wk.nrm and (once the stream gets there) wk.h_norms
+  int residual_norms() {
+    if (int rc = ama_kbatch_residual(prec, nk, nb, e->d.npw, e->d.pw_off, wk.X.p, wk.HX.p, wk.eps.as<double>(),
+                                     e->d.kin64, wk.nrm.as<double>(), nullptr, 0, nullptr, s))
+      return rc;
+    AMA_CUDA_TRY(cudaMemcpyAsync(wk.h_norms.p, wk.nrm.p, (size_t)nk * nb * sizeof(double), cudaMemcpyDeviceToHost, s));
+    return AMA_OK;
+  }
+
+  int run(const void* guess, double tol, int maxit, double* eps_out, void* x_out, double* norms_out, int* iterations) {
     const size_t blk = (size_t)total_pw * esz();
+    const size_t nkb = (size_t)nk * nb;
     for (Buf* b : {&wk.B, &wk.HB})
       if (int rc = b->need(blk * cap)) return rc;
     for (Buf* b : {&wk.X, &wk.HX, &wk.O1, &wk.O2, &wk.C, &wk.HN, &wk.X0})
       if (int rc = b->need(blk * nb)) return rc;
-    if (int rc = wk.nrm.need((size_t)nk * nb * sizeof(double))) return rc;
-    if (int rc = wk.rows.need((size_t)nk * nb * sizeof(int32_t))) return rc;
+    for (Buf* b : {&wk.nrm, &wk.eps})
+      if (int rc = b->need(nkb * sizeof(double))) return rc;
+    if (int rc = wk.rows.need(nkb * sizeof(int32_t))) return rc;
+    if (int rc = wk.tol.need(sizeof(double))) return rc;
+    if (int rc = wk.dev.need((size_t)nk * sizeof(double))) return rc;
+    for (Buf* b : {&wk.keep, &wk.valid})
+      if (int rc = b->need((size_t)nk * cap)) return rc;
+    if (int rc = wk.h_norms.need(nkb * sizeof(double))) return rc;
+    if (int rc = wk.h_keep.need(nkb)) return rc;
+    if (int rc = wk.h_dev.need((size_t)nk * sizeof(double))) return rc;
+    if (int rc = wk.h_tol.need(sizeof(double))) return rc;
+    double* h_norms = wk.h_norms.as<double>();
+    const uint8_t* h_keep = wk.h_keep.as<uint8_t>();
+    *wk.h_tol.as<double>() = tol;
+    AMA_CUDA_TRY(cudaMemcpyAsync(wk.tol.p, wk.h_tol.p, sizeof(double), cudaMemcpyHostToDevice, s));
+
     // the guess is usually the previous step's orthonormal orbitals: polish them without a
     // decomposition, else decompose the overlap (and reject a rank-deficient start)
-    std::vector<uint8_t> keep((size_t)nk * nb, 1);
-    bool ok = false;
-    if (int rc = lowdin_rows(const_cast<void*>(guess), nb, keep, wk.X0.p, &ok)) return rc;
-    if (!ok) {
-      if (int rc = orthonormal_rows(const_cast<void*>(guess), nb, 1e-10, false, wk.X0.p, keep)) return rc;
-      for (uint8_t k : keep)
-        AMA_REQUIRE(k, AMA_ERR_ARG, "the starting block of some k-point is rank deficient");
+    void* start = const_cast<void*>(guess);
+    AMA_CUDA_TRY(cudaMemsetAsync(wk.keep.p, 1, nkb, s));
+    if (int rc = lowdin_measure(start, nb)) return rc;
+    AMA_CUDA_TRY(cudaMemcpyAsync(wk.h_dev.p, wk.dev.p, (size_t)nk * sizeof(double), cudaMemcpyDeviceToHost, s));
+    AMA_CUDA_TRY(cudaStreamSynchronize(s));
+    const int steps0 = newton_schulz_steps();
+    if (steps0 >= 0) {
+      if (int rc = lowdin_apply(start, nb, steps0, wk.X0.p)) return rc;
+    } else {
+      if (int rc = orthonormal_rows(start, nb, 1e-10, false, wk.X0.p)) return rc;
+      AMA_CUDA_TRY(cudaMemcpyAsync(wk.h_keep.p, wk.keep.p, nkb, cudaMemcpyDeviceToHost, s));
+      AMA_CUDA_TRY(cudaStreamSynchronize(s));
+      for (size_t q = 0; q < nkb; ++q)
+        AMA_REQUIRE(h_keep[q], AMA_ERR_ARG, "the starting block of some k-point is rank deficient");
     }
     if (int rc = apply(wk.X0.p, nb, wk.HN.p)) return rc;
     if (int rc = copy_rows(wk.X0.p, nb, 0, wk.B.p, cap, 0, nb)) return rc;
     if (int rc = copy_rows(wk.HN.p, nb, 0, wk.HB.p, cap, 0, nb)) return rc;
-    std::fill(valid.begin(), valid.end(), 0);
-    for (int k = 0; k < nk; ++k)
-      for (int i = 0; i < nb; ++i) valid[(size_t)k * cap + i] = 1;
+    if (int rc = valid_prefix(nb)) return rc;
     int m = nb;
-    if (int rc = rayleigh_ritz(m, eps)) return rc;
-    std::vector<double> norms((size_t)nk * nb, INFINITY);
-    std::vector<int32_t> rows((size_t)nk * nb);
-    std::vector<uint8_t> keep1, keep2;
+    if (int rc = rayleigh_ritz(m)) return rc;
+    std::fill(h_norms, h_norms + nkb, INFINITY);
+    if (maxit >= 1)
+      if (int rc = residual_norms()) return rc;
+    AMA_CUDA_TRY(cudaStreamSynchronize(s));
+
     int it = 0;
     for (it = 1; it <= maxit; ++it) {
-      if (int rc = ama_kbatch_residual(prec, nk, nb, e->d.npw, e->d.pw_off, wk.X.p, wk.HX.p, eps, e->d.kin64,
-                                       wk.nrm.as<double>(), nullptr, 0, nullptr, s))
-        return rc;
-      AMA_CUDA_TRY(cudaMemcpyAsync(norms.data(), wk.nrm.p, norms.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
-      AMA_CUDA_TRY(cudaStreamSynchronize(s));
+      // h_norms: the residual norms of the current Ritz pairs
       int nn = 0;
       for (int k = 0; k < nk; ++k) {
         int c = 0;
-        for (int b = 0; b < nb; ++b) {
-          const bool act = norms[(size_t)k * nb + b] > tol;
-          rows[(size_t)k * nb + b] = act ? c++ : -1;
-        }
+        for (int b = 0; b < nb; ++b) c += h_norms[(size_t)k * nb + b] > tol;
         nn = std::max(nn, c);
       }
       if (nn == 0) break;
-      AMA_CUDA_TRY(cudaMemcpyAsync(wk.rows.p, rows.data(), rows.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
-      // rows of k-points with fewer active bands stay zero (and are dropped by the rank test)
-      AMA_CUDA_TRY(cudaMemsetAsync(wk.C.p, 0, blk * nn, s));
-      if (int rc = ama_kbatch_residual(prec, nk, nb, e->d.npw, e->d.pw_off, wk.X.p, wk.HX.p, eps, e->d.kin64,
-                                       wk.nrm.as<double>(), wk.rows.as<int32_t>(), nn, wk.C.p, s))
-        return rc;
-      if (int rc = wk.t.need((size_t)nk * nn * m * esz())) return rc;
-      for (int pass = 0; pass < 2; ++pass) {
-        const AmaKOperand top = op(wk.t.p, 0, 0, 0, m, (int64_t)nn * m);
-        if (int rc = gemm(1, nn, m, -1, op(wk.C.p, nn, 0, 1), op(wk.B.p, cap, 0, 1), top)) return rc;
-        if (int rc = gemm(0, nn, -1, m, top, op(wk.B.p, cap, 0, 1), op(wk.C.p, nn, 0, 1), -1.0, 1.0)) return rc;
-      }
-      if (int rc = orthonormal_rows(wk.C.p, nn, 1e-7, true, wk.O1.p, keep1)) return rc;
-      if (std::none_of(keep1.begin(), keep1.end(), [](uint8_t v) { return v != 0; })) break;  // all dependent
-      void* fresh = wk.O1.p;
-      const std::vector<uint8_t>* kept = &keep1;
-      if (int rc = lowdin_rows(wk.O1.p, nn, keep1, wk.O2.p, &ok)) return rc;
-      if (ok) {
-        fresh = wk.O2.p;
-      } else {
-        if (int rc = orthonormal_rows(wk.O1.p, nn, 0.5, false, wk.O2.p, keep2)) return rc;
-        fresh = wk.O2.p;
-        kept = &keep2;
-      }
-      if (int rc = apply(fresh, nn, wk.HN.p)) return rc;
-      if (int rc = copy_rows(fresh, nn, 0, wk.B.p, cap, m, nn)) return rc;
-      if (int rc = copy_rows(wk.HN.p, nn, 0, wk.HB.p, cap, m, nn)) return rc;
-      for (int k = 0; k < nk; ++k)
-        for (int i = 0; i < nn; ++i) valid[(size_t)k * cap + m + i] = (*kept)[(size_t)k * nn + i];
-      m += nn;
-      if (int rc = rayleigh_ritz(m, eps)) return rc;
-      if (m + nb > max_sub) {  // collapse onto the Ritz vectors
-        if (int rc = copy_rows(wk.X.p, nb, 0, wk.B.p, cap, 0, nb)) return rc;
-        if (int rc = copy_rows(wk.HX.p, nb, 0, wk.HB.p, cap, 0, nb)) return rc;
-        std::fill(valid.begin(), valid.end(), 0);
-        for (int k = 0; k < nk; ++k)
-          for (int i = 0; i < nb; ++i) valid[(size_t)k * cap + i] = 1;
-        m = nb;
-      }
+      const int m0 = m, m1 = m + nn;
+      // segment 1: corrections of the active bands, two projections off the basis, the rank
+      // test (-> O1, wk.keep) and the survivors' overlap (-> wk.g, wk.dev); rows of k-points
+      // with fewer active bands stay zero and are dropped by the rank test
+      int rc = segment(key(1, m0, nn, 0, 0), nn <= kJacobiMax, [&]() -> int {
+        active_rows_kernel<<<(nk + kSmT - 1) / kSmT, kSmT, 0, s>>>(wk.nrm.as<double>(), wk.tol.as<double>(), nk, nb,
+                                                                  wk.rows.as<int32_t>());
+        AMA_CHECK_LAUNCH();
+        AMA_CUDA_TRY(cudaMemsetAsync(wk.C.p, 0, blk * nn, s));
+        if (int r = ama_kbatch_residual(prec, nk, nb, e->d.npw, e->d.pw_off, wk.X.p, wk.HX.p, wk.eps.as<double>(),
+                                        e->d.kin64, wk.nrm.as<double>(), wk.rows.as<int32_t>(), nn, wk.C.p, s))
+          return r;
+        if (int r = wk.t.need((size_t)nk * nn * m0 * esz())) return r;
+        for (int pass = 0; pass < 2; ++pass) {
+          const AmaKOperand top = op(wk.t.p, 0, 0, 0, m0, (int64_t)nn * m0);
+          if (int r = gemm(1, nn, m0, -1, op(wk.C.p, nn, 0, 1), op(wk.B.p, cap, 0, 1), top)) return r;
+          if (int r = gemm(0, nn, -1, m0, top, op(wk.B.p, cap, 0, 1), op(wk.C.p, nn, 0, 1), -1.0, 1.0)) return r;
+        }
+        if (int r = orthonormal_rows(wk.C.p, nn, 1e-7, true, wk.O1.p)) return r;
+        if (int r = lowdin_measure(wk.O1.p, nn)) return r;
+        AMA_CUDA_TRY(cudaMemcpyAsync(wk.h_keep.p, wk.keep.p, (size_t)nk * nn, cudaMemcpyDeviceToHost, s));
+        AMA_CUDA_TRY(cudaMemcpyAsync(wk.h_dev.p, wk.dev.p, (size_t)nk * sizeof(double), cudaMemcpyDeviceToHost, s));
+        return AMA_OK;
+      });
+      if (rc) return rc;
+      AMA_CUDA_TRY(cudaStreamSynchronize(s));
+      if (std::none_of(h_keep, h_keep + (size_t)nk * nn, [](uint8_t v) { return v != 0; })) break;  // all dependent
+      const int steps = newton_schulz_steps();
+      const bool collapse = m1 + nb > max_sub, tail = it < maxit;
+      // segment 2: second orthonormalisation (-> O2, wk.keep), H on the new block, the basis
+      // extended, Rayleigh-Ritz, the collapse onto the Ritz vectors when one more block would
+      // not fit, and the next iteration's residual norms
+      rc = segment(key(2, m0, nn, steps, tail), m1 <= kJacobiMax, [&]() -> int {
+        if (steps >= 0) {
+          if (int r = lowdin_apply(wk.O1.p, nn, steps, wk.O2.p)) return r;
+        } else {
+          if (int r = orthonormal_rows(wk.O1.p, nn, 0.5, false, wk.O2.p)) return r;
+        }
+        if (int r = apply(wk.O2.p, nn, wk.HN.p)) return r;
+        if (int r = copy_rows(wk.O2.p, nn, 0, wk.B.p, cap, m0, nn)) return r;
+        if (int r = copy_rows(wk.HN.p, nn, 0, wk.HB.p, cap, m0, nn)) return r;
+        valid_append_kernel<<<blocks_for((int64_t)nk * nn), kSmT, 0, s>>>(wk.valid.as<uint8_t>(), wk.keep.as<uint8_t>(),
+                                                                          nk, cap, m0, nn);
+        AMA_CHECK_LAUNCH();
+        if (int r = rayleigh_ritz(m1)) return r;
+        if (collapse) {
+          if (int r = copy_rows(wk.X.p, nb, 0, wk.B.p, cap, 0, nb)) return r;
+          if (int r = copy_rows(wk.HX.p, nb, 0, wk.HB.p, cap, 0, nb)) return r;
+          if (int r = valid_prefix(nb)) return r;
+        }
+        return tail ? residual_norms() : AMA_OK;
+      });
+      if (rc) return rc;
+      m = collapse ? nb : m1;
+      AMA_CUDA_TRY(cudaStreamSynchronize(s));
     }
     if (it > maxit) it = maxit;
+    AMA_CUDA_TRY(cudaMemcpyAsync(eps_out, wk.eps.p, nkb * sizeof(double), cudaMemcpyDeviceToDevice, s));
     if (x_out != wk.X.p) AMA_CUDA_TRY(cudaMemcpyAsync(x_out, wk.X.p, blk * nb, cudaMemcpyDeviceToDevice, s));
-    if (norms_out)
-      AMA_CUDA_TRY(cudaMemcpyAsync(norms_out, norms.data(), norms.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+    if (norms_out) AMA_CUDA_TRY(cudaMemcpyAsync(norms_out, h_norms, nkb * sizeof(double), cudaMemcpyHostToDevice, s));
     AMA_CUDA_TRY(cudaStreamSynchronize(s));
     *iterations = it;
     return AMA_OK;
@@ -500,15 +670,36 @@ extern "C" int ama_davidson(AmaEngine* e, int32_t precision, int32_t spin, int32
   AMA_REQUIRE(nbands <= min_npw, AMA_ERR_SHAPE, "more bands than plane waves at some k-point");
   DavWork* wk = g_dav.here();
   AMA_REQUIRE(wk, AMA_ERR_UNSUPPORTED, "device index out of range");
-  cudaStream_t s = (cudaStream_t)stream;
+  // the iterations run on the library's own stream (the caller's may be the legacy default
+  // stream, which cannot be captured), after the work already queued on the caller's
+  if (!wk->stream) {
+    AMA_CUDA_TRY(cudaStreamCreateWithFlags(&wk->stream, cudaStreamNonBlocking));
+    AMA_CUDA_TRY(cudaEventCreateWithFlags(&wk->ready, cudaEventDisableTiming));
+  }
+  cudaStream_t s = wk->stream;
+  AMA_CUDA_TRY(cudaEventRecord(wk->ready, (cudaStream_t)stream));
+  AMA_CUDA_TRY(cudaStreamWaitEvent(s, wk->ready, 0));
   int it = 0, rc;
   if (precision == AMA_C64) {
-    Davidson<float> d(e, precision, spin, nbands, tc_min_npw > 0 && e->max_npw >= tc_min_npw, s, *wk);
+    Davidson<float> d(e, precision, spin, nbands, tc_min_npw > 0 && e->max_npw >= tc_min_npw, e->dav_graphs, s, *wk);
     rc = d.run(guess, tolerance, max_iterations, eigenvalues, x, norms, &it);
   } else {
-    Davidson<double> d(e, precision, spin, nbands, false, s, *wk);
+    Davidson<double> d(e, precision, spin, nbands, false, e->dav_graphs, s, *wk);
     rc = d.run(guess, tolerance, max_iterations, eigenvalues, x, norms, &it);
   }
+  if (rc) (void)cudaStreamSynchronize(s);  // nothing of this call is left running on an error
   *iterations = it;
   return rc;
+}
+
+extern "C" int ama_davidson_graph_stats(int64_t* captured, int64_t* replayed, int64_t* launched, int32_t reset) {
+  AMA_REQUIRE(captured && replayed && launched, AMA_ERR_ARG, "null argument");
+  DavWork* wk = g_dav.here();
+  AMA_REQUIRE(wk, AMA_ERR_UNSUPPORTED, "device index out of range");
+  GraphCache& gc = wk->graphs;
+  *captured = gc.captured;
+  *replayed = gc.replayed;
+  *launched = gc.launched;
+  if (reset) gc.captured = gc.replayed = gc.launched = 0;
+  return AMA_OK;
 }

@@ -55,6 +55,7 @@ namespace {
 
 template <typename T> cudaError_t grow(void** ptr, size_t* have, size_t need) {
   if (*have >= need) return cudaSuccess;
+  ama::bump_memory_epoch();
   if (*ptr) cudaFree(*ptr);
   *ptr = nullptr;
   *have = 0;
@@ -64,6 +65,7 @@ template <typename T> cudaError_t grow(void** ptr, size_t* have, size_t need) {
 }
 
 template <typename T> int upload(T** dst, const T* src, size_t count) {
+  ama::bump_memory_epoch();
   AMA_CUDA_TRY(cudaMalloc((void**)dst, std::max<size_t>(count, 1) * sizeof(T)));
   if (count) AMA_CUDA_TRY(cudaMemcpy(*dst, src, count * sizeof(T), cudaMemcpyHostToDevice));
   return AMA_OK;
@@ -1152,6 +1154,7 @@ int upload_twiddles(AmaEngine* e, int prec) {
 void free_grid_filters(AmaEngine* e);
 
 void free_engine(AmaEngine* e) {
+  ama::bump_memory_epoch();
   free_grid_filters(e);
   nl_tc_free(e);
   auto f = [](void* p) { if (p) cudaFree(p); };
@@ -1354,6 +1357,8 @@ extern "C" int ama_set_potential(AmaEngine* e, const double* v, int32_t nspin, v
   AMA_REQUIRE(nspin == e->nspin, AMA_ERR_SHAPE, "potential spin channels do not match the engine");
   cudaStream_t s = (cudaStream_t)stream;
   const int64_t N = e->N;
+  if ((!e->d.v64 && (e->precisions & (1u << AMA_C128))) || (!e->d.v32 && (e->precisions & (1u << AMA_C64))))
+    ama::bump_memory_epoch();
   if (!e->d.v64 && (e->precisions & (1u << AMA_C128)))
     AMA_CUDA_TRY(cudaMalloc((void**)&e->d.v64, (size_t)nspin * N * sizeof(double)));
   if (!e->d.v32 && (e->precisions & (1u << AMA_C64)))
@@ -1707,6 +1712,7 @@ __global__ void __launch_bounds__(kFftThreads) grid_g3_axpy_kernel(GridView g, c
 
 namespace {
 void free_grid_filters(AmaEngine* e) {
+  ama::bump_memory_epoch();
   for (double*& p : e->grid_filt) {
     if (p) cudaFree(p);
     p = nullptr;
@@ -1719,6 +1725,7 @@ void free_grid_filters(AmaEngine* e) {
 int ensure_grid_work(AmaEngine* e, int fields = 1) {
   const size_t need = (size_t)fields * e->N * sizeof(double2);
   if (e->grid_work_bytes >= need) return AMA_OK;
+  ama::bump_memory_epoch();
   if (e->grid_work) cudaFree(e->grid_work);
   e->grid_work = nullptr;
   e->grid_work_bytes = 0;
@@ -1755,6 +1762,7 @@ extern "C" int ama_set_grid_filter(AmaEngine* e, int32_t slot, const double* fil
     }
   }
   if (int rc = require_engine_device(e)) return rc;
+  if (!e->grid_filt[slot]) ama::bump_memory_epoch();
   if (!e->grid_filt[slot]) AMA_CUDA_TRY(cudaMalloc((void**)&e->grid_filt[slot], (size_t)e->N * sizeof(double)));
   AMA_CUDA_TRY(cudaMemcpy(e->grid_filt[slot], perm.data(), (size_t)e->N * sizeof(double), cudaMemcpyHostToDevice));
   return AMA_OK;
@@ -1886,6 +1894,7 @@ extern "C" int ama_grid_divergence(AmaEngine* e, const double* cell, const doubl
 
 extern "C" int ama_engine_option(AmaEngine* e, int32_t option, int32_t value) {
   AMA_REQUIRE(e, AMA_ERR_ARG, "null engine");
+  if (option != 4) ama::bump_memory_epoch();  // captured graphs hold the previous kernels and shapes
   switch (option) {
     case 0:  // nonlocal products of the complex64 path on the tensor cores (1) or SIMT (0)
       e->use_tc = value != 0;
@@ -1914,6 +1923,9 @@ extern "C" int ama_engine_option(AmaEngine* e, int32_t option, int32_t value) {
       e->ac_threads[AMA_C64] = e->ac_threads_of[AMA_C64][value];
       return AMA_OK;
     }
+    case 4:  // ama_davidson: iteration segments replayed as CUDA graphs (1, default) or launched (0)
+      e->dav_graphs = value != 0;
+      return AMA_OK;
     default:
       ama::set_error("unknown engine option");
       return AMA_ERR_ARG;

@@ -84,6 +84,7 @@ struct AmaEngine {
   int ac_threads[2] = {256, 256};        // [prec] threads per CTA of the selected stages A and C
   NlTcState tc;
   bool use_tc = true;
+  bool dav_graphs = true;  // ama_davidson replays recurring iteration segments as CUDA graphs
   // FP64 grid transforms (Hartree, Kerker): reciprocal-space filters in the engine's
   // permuted order, and the complex work grid of ama_grid_filter / ama_grid_fft_forward.
   // Both live on the engine's device; calls on one engine from different streams race on

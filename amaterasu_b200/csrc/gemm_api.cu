@@ -40,6 +40,7 @@ int zgemm_impl(int form, int m, int n, int k, const double* alpha, const void* a
   if (splits > 1) {
     const size_t need = (size_t)batch * splits * pstride * sizeof(double2);
     if (g_partial.bytes < need) {
+      bump_memory_epoch();
       if (g_partial.ptr) cudaFree(g_partial.ptr);
       g_partial.ptr = nullptr; g_partial.bytes = 0;
       AMA_CUDA_TRY(cudaMalloc(&g_partial.ptr, need));
@@ -141,6 +142,7 @@ int kbatch_impl(int form, int nk, int m, int n, int k, const int32_t* npw, const
   if (splits > 1) {
     const size_t need = (size_t)nk * splits * pstride * sizeof(double2);
     if (g_partial.bytes < need) {
+      bump_memory_epoch();
       if (g_partial.ptr) cudaFree(g_partial.ptr);
       g_partial.ptr = nullptr; g_partial.bytes = 0;
       AMA_CUDA_TRY(cudaMalloc(&g_partial.ptr, need));

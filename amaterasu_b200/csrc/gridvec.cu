@@ -196,6 +196,7 @@ thread_local PerDevice<VecScratch> g_vec;
 int vec_scratch(VecScratch** out) {
   VecScratch* v = g_vec.here();
   AMA_REQUIRE(v, AMA_ERR_CUDA, "grid vectors: no usable current CUDA device");
+  if (!v->partial || !v->sums) bump_memory_epoch();
   if (!v->partial) AMA_CUDA_TRY(cudaMalloc((void**)&v->partial, sizeof(double) * kPartialCtas * kMaxPairs));
   if (!v->sums) AMA_CUDA_TRY(cudaMalloc((void**)&v->sums, sizeof(double) * 8));
   *out = v;

@@ -856,6 +856,7 @@ int eig_scratch(int n, int nvec, EigScratch** out, EigLayout* L) {
   AMA_REQUIRE(sc, AMA_ERR_CUDA, "eigensolver: no usable current CUDA device");
   const size_t need = layout(nullptr, n, nvec).total;
   if (sc->bytes < need) {
+    bump_memory_epoch();
     if (sc->base) cudaFree(sc->base);
     sc->base = nullptr;
     sc->bytes = 0;
@@ -863,6 +864,7 @@ int eig_scratch(int n, int nvec, EigScratch** out, EigLayout* L) {
     sc->bytes = need;
   }
   if (!sc->status) {
+    bump_memory_epoch();
     AMA_CUDA_TRY(cudaMalloc((void**)&sc->status, sizeof(int)));
     AMA_CUDA_TRY(cudaMemset(sc->status, 0, sizeof(int)));
     int dev = 0;
@@ -1049,6 +1051,7 @@ extern "C" int ama_potrf_inv(int32_t n, void* matrices, int32_t batch, void* str
   AMA_REQUIRE(n >= 1 && batch >= 1, AMA_ERR_SHAPE, "bad sizes");
   CholScratch* cs = g_chol.here();
   AMA_REQUIRE(cs, AMA_ERR_CUDA, "inverse Cholesky: no usable current CUDA device");
+  if (!cs->flag) bump_memory_epoch();
   if (!cs->flag) AMA_CUDA_TRY(cudaMalloc((void**)&cs->flag, sizeof(int)));
   cudaStream_t s = (cudaStream_t)stream;
   AMA_CUDA_TRY(cudaMemsetAsync(cs->flag, 0, sizeof(int), s));

@@ -153,6 +153,7 @@ int make_map(CUtensorMap* map, const float* base, int x, int y, int z, int box_y
 
 int grow(float** p, size_t* have, size_t need) {
   if (*have >= need) return AMA_OK;
+  ama::bump_memory_epoch();
   if (*p) cudaFree(*p);
   *p = nullptr;
   *have = 0;
@@ -174,6 +175,7 @@ int nl_tc_setup(AmaEngine* e) {
   t.mp = round_up(2 * e->max_npw, kBM);
   const size_t bx = (size_t)e->nk * t.p2 * t.kp * sizeof(float);
   const size_t dx = (size_t)e->nk * t.mp * t.k2 * sizeof(float);
+  ama::bump_memory_epoch();
   for (int h = 0; h < 2; ++h) {
     AMA_CUDA_TRY(cudaMalloc((void**)&t.bx[h], bx));
     AMA_CUDA_TRY(cudaMalloc((void**)&t.dxt[h], dx));
@@ -294,6 +296,7 @@ int nl_tc_apply(AmaEngine* e, int k_first, int k_count, int nbands, float2* hpsi
 
 void nl_tc_free(AmaEngine* e) {
   NlTcState& t = e->tc;
+  ama::bump_memory_epoch();
   auto f = [](void* p) { if (p) cudaFree(p); };
   for (int h = 0; h < 2; ++h) { f(t.bx[h]); f(t.dxt[h]); }
   f(t.psi[0]);

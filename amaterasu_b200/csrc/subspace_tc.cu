@@ -206,6 +206,7 @@ struct Buf {
   size_t bytes = 0;
   int grow(size_t need) {
     if (bytes >= need) return AMA_OK;
+    bump_memory_epoch();
     if (p) cudaFree(p);
     p = nullptr;
     bytes = 0;
@@ -229,6 +230,7 @@ int ensure_err() {
   AMA_REQUIRE(gt, AMA_ERR_CUDA, "tensor-core subspace GEMM: no usable current CUDA device");
   TcScratch& g_tc = *gt;
   if (!g_tc.err) {
+    bump_memory_epoch();
     AMA_CUDA_TRY(cudaMalloc((void**)&g_tc.err, sizeof(int)));
     AMA_CUDA_TRY(cudaMemset(g_tc.err, 0, sizeof(int)));
   }

@@ -166,6 +166,7 @@ extern "C" int ama_residual_precondition(int32_t precision, int32_t nbands, int3
     AMA_REQUIRE(gm, AMA_ERR_CUDA, "no usable current CUDA device");
     MapScratch& g_map = *gm;
     if (g_map.n < nbands) {
+      bump_memory_epoch();
       if (g_map.ptr) cudaFree(g_map.ptr);
       g_map.ptr = nullptr; g_map.n = 0;
       AMA_CUDA_TRY(cudaMalloc((void**)&g_map.ptr, sizeof(int) * nbands));

@@ -238,6 +238,7 @@ extern "C" int ama_xc_gga(AmaEngine* e, int32_t functional, int32_t nspin, const
   AMA_REQUIRE(scp, AMA_ERR_UNSUPPORTED, "device index out of range");
   XcScratch& sc = *scp;
   if (sc.bytes < need) {
+    bump_memory_epoch();
     if (sc.buf) AMA_CUDA_TRY(cudaFree(sc.buf));
     sc.buf = nullptr;
     sc.bytes = 0;

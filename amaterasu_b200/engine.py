@@ -140,6 +140,11 @@ class DeviceEngine:
         column. Raises NotImplementedError when the variant is not compiled for this grid."""
         call("ama_engine_option", self.handle, 3, int(variant))
 
+    def set_davidson_graphs(self, on: bool) -> None:
+        """ama_davidson on this engine: replay recurring iteration segments as CUDA graphs
+        (True, the default) or launch every kernel (False). The results are the same."""
+        call("ama_engine_option", self.handle, 4, 1 if on else 0)
+
     def tc_status(self) -> int:
         code = ct.c_int32(0)
         call("ama_tc_status", self.handle, ct.byref(code))

@@ -301,6 +301,7 @@ def run_scf(system, config: Config | None = None, *, logger=None, wavefunctions=
                     bd = BatchedDavidson(system, nb, orb.dtype, tensor_cores=config.engine.tc_subspace,
                                          tc_min_npw=config.engine.tc_min_npw)
                     system._bd_cache = {**getattr(system, "_bd_cache", {}), key: bd}
+                bd.graphs = config.engine.davidson_graphs
                 eps, X, _, _ = bd.run(H, orb.packed[spin], tolerance=tol, max_iterations=maxit, spin=spin)
                 eigenvalues[spin] = eps
                 orb.packed[spin].copy_(X)

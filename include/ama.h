@@ -80,6 +80,8 @@ AMA_API int ama_engine_destroy(AmaEngine* engine);
  *             variant: 0 shared-memory y passes, 1 y transforms in registers with four
  *             threads per column (n2 a multiple of 4 on a compile-time grid);
  *             AMA_ERR_UNSUPPORTED when the variant is not compiled for the grid.
+ *   option 4: ama_davidson replays recurring iteration segments as CUDA graphs (value 1,
+ *             default) or launches every kernel (value 0); the results are the same.
  * amaterasu_b200.autotune times the variants and keeps the fastest. */
 AMA_API int ama_engine_option(AmaEngine* engine, int32_t option, int32_t value);
 
@@ -248,11 +250,22 @@ AMA_API int ama_kbatch_residual(int32_t precision, int32_t nk, int32_t nbands, c
  * (nbands, npw_k) block per k-point back to back, in the precision's complex type (x may be
  * guess). eigenvalues, norms: device FP64 [nk][nbands] (norms may be NULL); iterations: host.
  * tc_min_npw > 0 routes the complex64 plane-wave products to the tensor cores when the
- * largest sphere has at least that many plane waves (0: never). The host synchronises three
- * times per iteration. AMA_ERR_ARG for a rank-deficient start. */
+ * largest sphere has at least that many plane waves (0: never). The iterations run on the
+ * library's own stream after the work queued on `stream`; the call returns when its results
+ * are written. The host synchronises twice per iteration (the active bands; the rank test
+ * and the orthonormalisation's admissibility); the launches between two synchronisations
+ * depend only on the basis size, the block width and the Newton-Schulz step count, and with
+ * engine option 4 on (the default) such a segment is captured as a CUDA graph on its second
+ * occurrence and replayed afterwards (segments with eigensolves above order 80 are launched
+ * directly). AMA_ERR_ARG for a rank-deficient start. */
 AMA_API int ama_davidson(AmaEngine* engine, int32_t precision, int32_t spin, int32_t nbands, const void* guess,
                          double tolerance, int32_t max_iterations, int32_t tc_min_npw, double* eigenvalues,
                          void* x, double* norms, int32_t* iterations, void* stream);
+
+/* ama_davidson's iteration segments on the calling host thread and current device: captured
+ * as CUDA graphs, replayed from a graph, launched kernel by kernel (counts since the last
+ * reset; reset != 0 zeroes them after reading). No counterpart in the reference. */
+AMA_API int ama_davidson_graph_stats(int64_t* captured, int64_t* replayed, int64_t* launched, int32_t reset);
 
 /* Copy nrows rows per k-point between packed per-k blocks (block k at rows_per_k*pw_off[k],
  * rows of npw_k elements, starting at row row0). */
