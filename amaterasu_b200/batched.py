@@ -6,9 +6,10 @@ projections off the basis, drop directions below 1e-7, orthonormalise, extend, c
 subspace_factor * nbands). All k-points advance together: every step is one launch over all
 k (ragged plane-wave counts), H.psi runs on every k's new block in one engine call, the
 small per-k problems are solved by the batched Jacobi eigensolver, and the host synchronises
-three times per iteration for the whole set instead of per k. ``BatchedDavidson.run`` runs
-the loop inside the library (``ama_davidson``, csrc/davidson.cu); ``run_python`` is the same
-loop with its host logic written here over the same kernels, kept as its check.
+for the whole set instead of per k. ``BatchedDavidson.run`` runs the loop inside the library
+(``ama_davidson``, csrc/davidson.cu: two synchronisations per iteration, the segments between
+them replayed as CUDA graphs once they recur); ``run_python`` is the same loop with its host
+logic written here over the same kernels (three synchronisations), kept as its check.
 
 Storage: the basis of k-point k is a (cap, npw_k) block at cap * pw_off[k]; every k carries
 the same number of rows. When a k-point has fewer new directions than the others (fewer
