@@ -1,6 +1,6 @@
 """Data generation, training and evaluation of the learned start density.
 
-    python -m amaterasu_b200.learned_pipeline all --family si8 --train 48 --test 12 --out DIR
+    python -m amaterasu_b200.learned_pipeline all --family si8 --train 2000 --test 200 --workers 8 --out DIR
     python -m amaterasu_b200.learned_pipeline all --family si64 --train 32 --test 4 --out DIR
     python -m amaterasu_b200.learned_pipeline all --family si215 --train 16 --test 2 --init W --out DIR
 
@@ -123,17 +123,45 @@ def run_cell(seed, pseudo, *, family="si8", ecut=15.0, density=None, precision="
                 strain=strain_of(system.cell, ref / BOHR_IN_ANGSTROM))
 
 
-def generate(seeds, out_file, **kw):
+def _save_dataset(out_file, rows):
+    np.savez_compressed(out_file, n0=np.stack([r["n0"] for r in rows]), nconv=np.stack([r["nconv"] for r in rows]),
+                        strain=np.stack([r["strain"] for r in rows]), seeds=np.array([r["seed"] for r in rows]),
+                        iterations=np.array([r["iterations"] for r in rows]),
+                        seconds=np.array([r["seconds"] for r in rows]))
+
+
+def _generate_rows(seeds, kw):
     pseudo = _pseudo()
     rows = []
     for s in seeds:
         r = run_cell(s, pseudo, **kw)
         rows.append(r)
         print(f"cell {s}: grid {r['grid']} {r['iterations']} iterations {r['seconds']:.1f} s", flush=True)
-    np.savez_compressed(out_file, n0=np.stack([r["n0"] for r in rows]), nconv=np.stack([r["nconv"] for r in rows]),
-                        strain=np.stack([r["strain"] for r in rows]), seeds=np.array(seeds),
-                        iterations=np.array([r["iterations"] for r in rows]),
-                        seconds=np.array([r["seconds"] for r in rows]))
+    return rows
+
+
+def _shards(seeds, workers):
+    return [list(seeds[i::workers]) for i in range(workers) if seeds[i::workers]]
+
+
+def _pool_map(fn, shards, kw):
+    """fn(shard, kw) for every shard, each in its own spawned process (one CUDA context each,
+    all on the current device: the cells are small, so several SCFs share the GPU)."""
+    import multiprocessing as mp
+    with mp.get_context("spawn").Pool(len(shards)) as pool:
+        return pool.starmap(fn, [(s, kw) for s in shards])
+
+
+def generate(seeds, out_file, workers=1, **kw):
+    """Converge every seed's cell; write the (n0, strain) -> n_conv samples to out_file in
+    seed order. ``workers`` > 1 runs that many processes over interleaved seed shards."""
+    seeds = list(seeds)
+    if workers > 1:
+        rows = [r for part in _pool_map(_generate_rows, _shards(seeds, workers), kw) for r in part]
+    else:
+        rows = _generate_rows(seeds, kw)
+    rows.sort(key=lambda r: seeds.index(r["seed"]))
+    _save_dataset(out_file, rows)
     return rows
 
 
@@ -160,7 +188,19 @@ def learned_start(weights, family: str):
     return LearnedStart(net, reference_cell(family) / BOHR_IN_ANGSTROM, grid=FAMILIES[family]["grid"])
 
 
-def evaluate(weights, seeds, *, family="si8", **kw):
+def _evaluate_rows(seeds, kw):
+    kw = dict(kw)
+    return evaluate(kw.pop("weights"), seeds, **kw)
+
+
+def evaluate(weights, seeds, *, family="si8", workers=1, **kw):
+    """Converge every held-out cell from the superposition and from the network's start.
+    ``workers`` > 1 runs that many processes over interleaved seed shards; the rows come
+    back in seed order."""
+    seeds = list(seeds)
+    if workers > 1:
+        parts = _pool_map(_evaluate_rows, _shards(seeds, workers), dict(kw, weights=str(weights), family=family))
+        return sorted((r for part in parts for r in part), key=lambda r: seeds.index(r["seed"]))
     pseudo = _pseudo()
     learned = learned_start(weights, family)
     rows = []
@@ -195,17 +235,18 @@ def main():
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--init", default=None, help="start the fit from these weights")
     ap.add_argument("--out", default="learned_out")
+    ap.add_argument("--workers", type=int, default=1, help="processes converging cells side by side")
     args = ap.parse_args()
     out = Path(args.out)
     out.mkdir(parents=True, exist_ok=True)
     train_seeds = list(range(1000, 1000 + args.train))
     test_seeds = list(range(5000, 5000 + args.test))
     if args.stage in ("generate", "all"):
-        generate(train_seeds, out / "dataset.npz", family=args.family)
+        generate(train_seeds, out / "dataset.npz", workers=args.workers, family=args.family)
     if args.stage in ("fit", "all"):
         fit(out / "dataset.npz", out / "density_net.npz", epochs=args.epochs, lr=args.lr, init=args.init)
     if args.stage in ("evaluate", "all"):
-        summary = summarize(evaluate(out / "density_net.npz", test_seeds, family=args.family))
+        summary = summarize(evaluate(out / "density_net.npz", test_seeds, family=args.family, workers=args.workers))
         summary["family"] = args.family
         (out / "evaluation.json").write_text(json.dumps(summary, indent=1))
         print(json.dumps({k: v for k, v in summary.items() if k != "rows"}), flush=True)
