@@ -1087,7 +1087,7 @@ int hpsi_impl(AmaEngine* e, int k_first, int k_count, int nbands, int spin, cons
     int maxnpw = 0;
     for (int k = k_first; k < k_first + k_count; ++k) maxnpw = std::max(maxnpw, e->npw[k]);
     // split the long npw reduction so that the tile grid covers the GPU several times
-    const int tiles = ((nbands + kBM - 1) / kBM) * ((e->nproj + kBN - 1) / kBN) * k_count;
+    const int tiles = (int)std::min<int64_t>(gemm_tile_count<T>(nbands, e->nproj, k_count), 1 << 30);
     int splits = std::max(1, std::min(64, (4 * 148 + tiles - 1) / tiles));
     splits = std::min(splits, std::max(1, maxnpw / 256));
     const int64_t pstride = (int64_t)nbands * e->nproj;
@@ -1424,7 +1424,7 @@ template <typename T>
 static int project_impl(AmaEngine* e, int k, int nbands, const void* psi, void* out, cudaStream_t s) {
   using C = cx_t<T>;
   const int p = std::is_same<T, float>::value ? AMA_C64 : AMA_C128;
-  const int tiles = ((nbands + kBM - 1) / kBM) * ((e->nproj + kBN - 1) / kBN);
+  const int tiles = (int)std::min<int64_t>(gemm_tile_count<T>(nbands, e->nproj, 1), 1 << 30);
   int splits = std::max(1, std::min(64, (4 * 148 + tiles - 1) / tiles));
   splits = std::min(splits, std::max(1, e->npw[k] / 256));
   const int64_t pstride = (int64_t)nbands * e->nproj;

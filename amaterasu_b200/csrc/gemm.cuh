@@ -191,14 +191,17 @@ cgemm_tile_kernel(Batch batch, int splits, cx_t<T> alpha, cx_t<T> beta, double2*
 }
 
 // FP64 complex GEMM on the FP64 tensor cores (mma.sync m8n8k4, DMMA): same forms, batches,
-// split-K and epilogue as cgemm_tile_kernel<double>. A CTA computes a 64 x 64 complex tile
-// with 8 warps (2 along M x 4 along N), each warp 32 x 16 complex = 4 x 2 blocks of 8 x 8.
-// The k-tile (8) is staged as separate real and imaginary planes, k-major with a 72-double
-// row pitch (the fragment loads of a warp then take the minimum two wavefronts), double
-// buffered with a register prefetch of the next tile. Per 8 x 8 block and k-step of 4:
+// split-K and epilogue as cgemm_tile_kernel<double>. A CTA computes a BM x BN complex tile
+// with 8 warps (WMW along M x 8/WMW along N); the 64 x 64 tile has 2 x 4 warps of 32 x 16
+// complex = 4 x 2 blocks of 8 x 8 each. The k-tile (8) is staged as separate real and
+// imaginary planes, k-major with a row pitch of BM + 8 (BN + 8) doubles, 8 modulo 16 (the
+// fragment loads of a warp then take the minimum two wavefronts), double buffered with a
+// register prefetch of the next tile. Per 8 x 8 block and k-step of 4:
 //   Re C += Ar Br + (-Ai) Bi,   Im C += Ar Bi + Ai Br   (four DMMAs).
+// The tensor cores compute the whole padded tile, so short operands (the Davidson's block
+// of at most 32 new directions, its small Gram and projection matrices) take a 32-row tile:
+// 32 x 128 (warps 1 x 8, the same 32 x 16 warp tile) or 32 x 32 (warps 2 x 4 of 16 x 8).
 constexpr int kDmmaBK = 8;
-constexpr int kDmmaPitch = kBM + 8;
 
 __device__ __forceinline__ void dmma_884(double (&c)[2], double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
@@ -206,32 +209,59 @@ __device__ __forceinline__ void dmma_884(double (&c)[2], double a, double b) {
                : "d"(a), "d"(b));
 }
 
-template <int FORM, class Batch>
-__global__ void __launch_bounds__(kGemmThreads)
+// The CTA tile of the FP64 kernel for a problem of at most max_m x max_n.
+struct DmmaTile {
+  int bm, bn;
+};
+inline DmmaTile dmma_tile(int max_m, int max_n) {
+  if (max_m <= 32 && max_n <= 64) return {32, 32};
+  if (max_m <= 32) return {32, 128};
+  return {64, 64};
+}
+
+// Tiles the launch of launch_cgemm<T> covers (split-K counts are sized from it).
+template <typename T> inline int64_t gemm_tile_count(int max_m, int max_n, int nbatch) {
+  int bm = kBM, bn = kBN;
+  if constexpr (std::is_same<T, double>::value) {
+    const DmmaTile t = dmma_tile(max_m, max_n);
+    bm = t.bm;
+    bn = t.bn;
+  }
+  return (int64_t)((max_m + bm - 1) / bm) * ((max_n + bn - 1) / bn) * nbatch;
+}
+
+template <int FORM, int BM, int BN, int WMW, class Batch>
+__global__ void __launch_bounds__(kGemmThreads, 2)
 zgemm_dmma_kernel(Batch batch, int splits, double2 alpha, double2 beta, double2* partial, int64_t partial_stride) {
   using C = double2;
-  constexpr int BK = kDmmaBK, P = kDmmaPitch;
-  constexpr int LA = BK * kBM / kGemmThreads, LB = BK * kBN / kGemmThreads;  // 2 and 2
-  __shared__ double Ar[2][BK][P], Ai[2][BK][P], Br[2][BK][P], Bi[2][BK][P];
+  constexpr int BK = kDmmaBK, PA = BM + 8, PB = BN + 8;
+  constexpr int WNW = kGemmThreads / 32 / WMW;
+  constexpr int WTM = BM / WMW, WTN = BN / WNW;  // warp tile
+  constexpr int IM = WTM / 8, JN = WTN / 8;      // 8 x 8 blocks per warp
+  constexpr int LA = BK * BM / kGemmThreads, LB = BK * BN / kGemmThreads;
+  static_assert(WTM % 8 == 0 && WTN % 8 == 0 && LA >= 1 && LB >= 1 && BK * BM % kGemmThreads == 0 &&
+                    BK * BN % kGemmThreads == 0 && PA % 16 == 8 && PB % 16 == 8,
+                "DMMA tile shape");
+  __shared__ double Ar[2][BK][PA], Ai[2][BK][PA], Br[2][BK][PB], Bi[2][BK][PB];
 
   const int z = blockIdx.z;
   const int bz = z / splits, sz = z % splits;
   const GemmProblem<C> p = batch(bz);
-  const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * kBN;
+  const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
   if (m0 >= p.m || n0 >= p.n) return;
   const int kchunk = ((p.k + splits - 1) / splits + BK - 1) / BK * BK;
   const int kbeg = sz * kchunk;
   const int kend = min(p.k, kbeg + kchunk);
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int wm = (warp & 1) * 32, wn = (warp >> 1) * 16;
+  const int wm = (warp % WMW) * WTM, wn = (warp / WMW) * WTN;
   const int fr = lane >> 2, fk = lane & 3;  // fragment row (m or n) and k of this lane
 
-  double cre[4][2][2], cim[4][2][2];
+  double cre[IM][JN][2], cim[IM][JN][2];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < IM; ++i)
 #pragma unroll
-    for (int j = 0; j < 2; ++j) cre[i][j][0] = cre[i][j][1] = cim[i][j][0] = cim[i][j][1] = 0.0;
+    for (int j = 0; j < JN; ++j) cre[i][j][0] = cre[i][j][1] = cim[i][j][0] = cim[i][j][1] = 0.0;
 
   C ra[LA], rb[LB];
   auto load_tile = [&](int k0) {
@@ -239,7 +269,7 @@ zgemm_dmma_kernel(Batch batch, int splits, double2 alpha, double2 beta, double2*
     for (int l = 0; l < LA; ++l) {
       const int e = tid + l * kGemmThreads;
       int mm, kk;
-      if (FORM == kCN) { mm = e % kBM; kk = e / kBM; }
+      if (FORM == kCN) { mm = e % BM; kk = e / BM; }
       else { kk = e % BK; mm = e / BK; }
       const int gm = m0 + mm, gk = k0 + kk;
       C v = make_double2(0.0, 0.0);
@@ -254,7 +284,7 @@ zgemm_dmma_kernel(Batch batch, int splits, double2 alpha, double2 beta, double2*
       const int e = tid + l * kGemmThreads;
       int nn, kk;
       if (FORM == kNC) { kk = e % BK; nn = e / BK; }
-      else { nn = e % kBN; kk = e / kBN; }
+      else { nn = e % BN; kk = e / BN; }
       const int gn = n0 + nn, gk = k0 + kk;
       C v = make_double2(0.0, 0.0);
       if (gn < p.n && gk < kend) {
@@ -269,7 +299,7 @@ zgemm_dmma_kernel(Batch batch, int splits, double2 alpha, double2 beta, double2*
     for (int l = 0; l < LA; ++l) {
       const int e = tid + l * kGemmThreads;
       int mm, kk;
-      if (FORM == kCN) { mm = e % kBM; kk = e / kBM; }
+      if (FORM == kCN) { mm = e % BM; kk = e / BM; }
       else { kk = e % BK; mm = e / BK; }
       Ar[buf][kk][mm] = ra[l].x;
       Ai[buf][kk][mm] = ra[l].y;
@@ -279,7 +309,7 @@ zgemm_dmma_kernel(Batch batch, int splits, double2 alpha, double2 beta, double2*
       const int e = tid + l * kGemmThreads;
       int nn, kk;
       if (FORM == kNC) { kk = e % BK; nn = e / BK; }
-      else { nn = e % kBN; kk = e / kBN; }
+      else { nn = e % BN; kk = e / BN; }
       Br[buf][kk][nn] = rb[l].x;
       Bi[buf][kk][nn] = rb[l].y;
     }
@@ -296,22 +326,22 @@ zgemm_dmma_kernel(Batch batch, int splits, double2 alpha, double2 beta, double2*
     if (more) load_tile(k0 + BK);
 #pragma unroll
     for (int ks = 0; ks < BK; ks += 4) {
-      double ar[4], ai[4], nai[4], br[2], bi[2];
+      double ar[IM], ai[IM], nai[IM], br[JN], bi[JN];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
+      for (int i = 0; i < IM; ++i) {
         ar[i] = Ar[buf][ks + fk][wm + 8 * i + fr];
         ai[i] = Ai[buf][ks + fk][wm + 8 * i + fr];
         nai[i] = -ai[i];
       }
 #pragma unroll
-      for (int j = 0; j < 2; ++j) {
+      for (int j = 0; j < JN; ++j) {
         br[j] = Br[buf][ks + fk][wn + 8 * j + fr];
         bi[j] = Bi[buf][ks + fk][wn + 8 * j + fr];
       }
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+      for (int i = 0; i < IM; ++i)
 #pragma unroll
-        for (int j = 0; j < 2; ++j) {
+        for (int j = 0; j < JN; ++j) {
           dmma_884(cre[i][j], ar[i], br[j]);
           dmma_884(cre[i][j], nai[i], bi[j]);
           dmma_884(cim[i][j], ar[i], bi[j]);
@@ -325,11 +355,11 @@ zgemm_dmma_kernel(Batch batch, int splits, double2 alpha, double2 beta, double2*
 
   // lane holds C[wm + 8 i + fr][wn + 8 j + 2 fk + t]
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
+  for (int i = 0; i < IM; ++i) {
     const int gm = m0 + wm + 8 * i + fr;
     if (gm >= p.m) continue;
 #pragma unroll
-    for (int j = 0; j < 2; ++j)
+    for (int j = 0; j < JN; ++j)
 #pragma unroll
       for (int t = 0; t < 2; ++t) {
         const int gn = n0 + wn + 8 * j + 2 * fk + t;
@@ -380,8 +410,19 @@ cudaError_t launch_cgemm(Batch batch, int nbatch, int max_m, int max_n, int spli
                          cudaStream_t stream) {
   dim3 grid((max_n + kBN - 1) / kBN, (max_m + kBM - 1) / kBM, nbatch * splits);
   if constexpr (std::is_same<T, double>::value) {  // FP64: the FP64 tensor cores
-    zgemm_dmma_kernel<FORM><<<grid, kGemmThreads, 0, stream>>>(batch, splits <= 1 ? 1 : splits, alpha, beta,
-                                                               splits <= 1 ? nullptr : partial, partial_stride);
+    const DmmaTile t = dmma_tile(max_m, max_n);
+    grid = dim3((max_n + t.bn - 1) / t.bn, (max_m + t.bm - 1) / t.bm, nbatch * splits);
+    const int sp = splits <= 1 ? 1 : splits;
+    double2* part = splits <= 1 ? nullptr : partial;
+    if (t.bm == 32 && t.bn == 32)
+      zgemm_dmma_kernel<FORM, 32, 32, 2><<<grid, kGemmThreads, 0, stream>>>(batch, sp, alpha, beta, part,
+                                                                          partial_stride);
+    else if (t.bm == 32)
+      zgemm_dmma_kernel<FORM, 32, 128, 1><<<grid, kGemmThreads, 0, stream>>>(batch, sp, alpha, beta, part,
+                                                                           partial_stride);
+    else
+      zgemm_dmma_kernel<FORM, 64, 64, 2><<<grid, kGemmThreads, 0, stream>>>(batch, sp, alpha, beta, part,
+                                                                          partial_stride);
     if (splits <= 1) return cudaGetLastError();
   } else {
     if (splits <= 1) {

@@ -30,7 +30,7 @@ int zgemm_impl(int form, int m, int n, int k, const double* alpha, const void* a
   using C = cx_t<T>;
   StridedBatch<C> sbch{(const C*)a, (const C*)b, (C*)c, m, n, k, lda, ldb, ldc, sa, sb, sc};
   const C al = mk<C>(alpha[0], alpha[1]), be = mk<C>(beta[0], beta[1]);
-  const int tiles = ((m + kBM - 1) / kBM) * ((n + kBN - 1) / kBN) * batch;
+  const int tiles = (int)std::min<int64_t>(gemm_tile_count<T>(m, n, batch), 1 << 30);
   int splits = std::max(1, std::min(32, (2 * 148 + tiles - 1) / tiles));
   splits = std::min(splits, std::max(1, k / 512));
   const int64_t pstride = (int64_t)m * n;
@@ -132,7 +132,7 @@ int kbatch_impl(int form, int nk, int m, int n, int k, const int32_t* npw, const
   // split a long (plane-wave) reduction when the tile grid alone does not fill the GPU
   int splits = 1;
   if (k < 0) {  // a slice shorter than one k-tile (few plane waves) just writes zeros
-    const int tiles = ((max_m + kBM - 1) / kBM) * ((max_n + kBN - 1) / kBN) * nk;
+    const int tiles = (int)std::min<int64_t>(gemm_tile_count<T>(max_m, max_n, nk), 1 << 30);
     splits = std::max(1, std::min(32, (2 * 148 + tiles - 1) / tiles));
   }
   const int64_t pstride = (int64_t)max_m * max_n;

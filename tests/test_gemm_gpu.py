@@ -1,6 +1,6 @@
 """SIMT complex GEMMs (ama_zgemm, ama_kbatch_zgemm) against FP64 products of the same
-operands, every form (NN, NC, CN), both precisions, odd sizes, split-K and ragged per-k
-batches, with alpha/beta.
+operands, every form (NN, NC, CN), both precisions, odd sizes, every tile shape of the
+FP64 tensor-core kernel, split-K and ragged per-k batches, with alpha/beta.
 
 Tolerances: complex128 1e-13, complex64 2e-6 of max|C| (the FP32 sums are flushed into FP64
 every 128 products, so the error does not grow with the reduction length).
@@ -30,7 +30,11 @@ def _tol(dtype):
 
 @pytest.mark.parametrize("dtype", [torch.complex64, torch.complex128])
 @pytest.mark.parametrize("form", [0, 1, 2])
-@pytest.mark.parametrize("m,n,k,batch", [(37, 53, 29, 3), (70, 65, 40000, 1), (128, 64, 600, 2)])
+# complex128 tile shapes: 64 x 64 (the first three and (33, 20)), 32 x 32 (m <= 32, n <= 64;
+# split-K at (20, 40)), 32 x 128 (m <= 32, n > 64)
+@pytest.mark.parametrize("m,n,k,batch", [(37, 53, 29, 3), (70, 65, 40000, 1), (128, 64, 600, 2), (33, 20, 50, 2),
+                                         (20, 40, 4615, 5), (32, 64, 1000, 1), (1, 1, 5, 1), (17, 300, 77, 2),
+                                         (32, 129, 4000, 1)])
 def test_zgemm_forms(dtype, form, m, n, k, batch):
     from amaterasu_b200._lib import AMA_C64, AMA_C128, call, load
     load()
