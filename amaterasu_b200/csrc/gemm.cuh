@@ -219,21 +219,24 @@ inline DmmaTile dmma_tile(int max_m, int max_n) {
   return {64, 64};
 }
 
-// Tiles the launch of launch_cgemm<T> covers (split-K counts are sized from it).
-template <typename T> inline int64_t gemm_tile_count(int max_m, int max_n, int nbatch) {
-  int bm = kBM, bn = kBN;
-  if constexpr (std::is_same<T, double>::value) {
-    const DmmaTile t = dmma_tile(max_m, max_n);
-    bm = t.bm;
-    bn = t.bn;
-  }
-  return (int64_t)((max_m + bm - 1) / bm) * ((max_n + bn - 1) / bn) * nbatch;
+// The CTA tile launch_cgemm<T> uses: the FP64 tensor-core kernel's choice for complex128,
+// and for complex64 too when at most 32 rows (complex64 operands staged in FP64; longer
+// ones take the 64 x 64 SIMT FP32 tile).
+template <typename T> inline DmmaTile gemm_tile(int max_m, int max_n) {
+  if (std::is_same<T, double>::value || max_m <= 32) return dmma_tile(max_m, max_n);
+  return {kBM, kBN};
 }
 
-template <int FORM, int BM, int BN, int WMW, class Batch>
+// Tiles the launch of launch_cgemm<T> covers (split-K counts are sized from it).
+template <typename T> inline int64_t gemm_tile_count(int max_m, int max_n, int nbatch) {
+  const DmmaTile t = gemm_tile<T>(max_m, max_n);
+  return (int64_t)((max_m + t.bm - 1) / t.bm) * ((max_n + t.bn - 1) / t.bn) * nbatch;
+}
+
+template <typename T, int FORM, int BM, int BN, int WMW, class Batch>
 __global__ void __launch_bounds__(kGemmThreads, 2)
 zgemm_dmma_kernel(Batch batch, int splits, double2 alpha, double2 beta, double2* partial, int64_t partial_stride) {
-  using C = double2;
+  using C = cx_t<T>;  // operands and result; staged, multiplied and summed in FP64
   constexpr int BK = kDmmaBK, PA = BM + 8, PB = BN + 8;
   constexpr int WNW = kGemmThreads / 32 / WMW;
   constexpr int WTM = BM / WMW, WTN = BN / WNW;  // warp tile
@@ -263,7 +266,7 @@ zgemm_dmma_kernel(Batch batch, int splits, double2 alpha, double2 beta, double2*
 #pragma unroll
     for (int j = 0; j < JN; ++j) cre[i][j][0] = cre[i][j][1] = cim[i][j][0] = cim[i][j][1] = 0.0;
 
-  C ra[LA], rb[LB];
+  double2 ra[LA], rb[LB];
   auto load_tile = [&](int k0) {
 #pragma unroll
     for (int l = 0; l < LA; ++l) {
@@ -272,10 +275,10 @@ zgemm_dmma_kernel(Batch batch, int splits, double2 alpha, double2 beta, double2*
       if (FORM == kCN) { mm = e % BM; kk = e / BM; }
       else { kk = e % BK; mm = e / BK; }
       const int gm = m0 + mm, gk = k0 + kk;
-      C v = make_double2(0.0, 0.0);
+      double2 v = make_double2(0.0, 0.0);
       if (gm < p.m && gk < kend) {
-        if (FORM == kCN) { v = p.a[(int64_t)gk * p.lda + gm]; v.y = -v.y; }
-        else v = p.a[(int64_t)gm * p.lda + gk];
+        const C x = FORM == kCN ? p.a[(int64_t)gk * p.lda + gm] : p.a[(int64_t)gm * p.lda + gk];
+        v = make_double2((double)x.x, FORM == kCN ? -(double)x.y : (double)x.y);
       }
       ra[l] = v;
     }
@@ -286,10 +289,10 @@ zgemm_dmma_kernel(Batch batch, int splits, double2 alpha, double2 beta, double2*
       if (FORM == kNC) { kk = e % BK; nn = e / BK; }
       else { nn = e % BN; kk = e / BN; }
       const int gn = n0 + nn, gk = k0 + kk;
-      C v = make_double2(0.0, 0.0);
+      double2 v = make_double2(0.0, 0.0);
       if (gn < p.n && gk < kend) {
-        if (FORM == kNC) { v = p.b[(int64_t)gn * p.ldb + gk]; v.y = -v.y; }
-        else v = p.b[(int64_t)gk * p.ldb + gn];
+        const C x = FORM == kNC ? p.b[(int64_t)gn * p.ldb + gk] : p.b[(int64_t)gk * p.ldb + gn];
+        v = make_double2((double)x.x, FORM == kNC ? -(double)x.y : (double)x.y);
       }
       rb[l] = v;
     }
@@ -364,14 +367,17 @@ zgemm_dmma_kernel(Batch batch, int splits, double2 alpha, double2 beta, double2*
       for (int t = 0; t < 2; ++t) {
         const int gn = n0 + wn + 8 * j + 2 * fk + t;
         if (gn >= p.n) continue;
-        const C sum = make_double2(cre[i][j][t], cim[i][j][t]);
+        const double2 sum = make_double2(cre[i][j][t], cim[i][j][t]);
         if (partial) {
           partial[(int64_t)z * partial_stride + (int64_t)gm * p.n + gn] = sum;
         } else {
           C* dst = p.c + (int64_t)gm * p.ldc + gn;
-          C r = cmul(alpha, sum);
-          if (beta.x != 0.0 || beta.y != 0.0) r = cadd(r, cmul(beta, *dst));
-          *dst = r;
+          double2 r = cmul(alpha, sum);
+          if (beta.x != 0.0 || beta.y != 0.0) {
+            const C d = *dst;
+            r = cadd(r, cmul(beta, make_double2((double)d.x, (double)d.y)));
+          }
+          *dst = mk<C>(r.x, r.y);
         }
       }
   }
@@ -409,20 +415,22 @@ cudaError_t launch_cgemm(Batch batch, int nbatch, int max_m, int max_n, int spli
                          cx_t<T> alpha, cx_t<T> beta, double2* partial, int64_t partial_stride,
                          cudaStream_t stream) {
   dim3 grid((max_n + kBN - 1) / kBN, (max_m + kBM - 1) / kBM, nbatch * splits);
-  if constexpr (std::is_same<T, double>::value) {  // FP64: the FP64 tensor cores
-    const DmmaTile t = dmma_tile(max_m, max_n);
+  const DmmaTile t = gemm_tile<T>(max_m, max_n);
+  if (std::is_same<T, double>::value || t.bm == 32) {  // the FP64 tensor cores
     grid = dim3((max_n + t.bn - 1) / t.bn, (max_m + t.bm - 1) / t.bm, nbatch * splits);
     const int sp = splits <= 1 ? 1 : splits;
     double2* part = splits <= 1 ? nullptr : partial;
+    const double2 al = make_double2((double)alpha.x, (double)alpha.y);
+    const double2 be = make_double2((double)beta.x, (double)beta.y);
     if (t.bm == 32 && t.bn == 32)
-      zgemm_dmma_kernel<FORM, 32, 32, 2><<<grid, kGemmThreads, 0, stream>>>(batch, sp, alpha, beta, part,
-                                                                          partial_stride);
+      zgemm_dmma_kernel<T, FORM, 32, 32, 2><<<grid, kGemmThreads, 0, stream>>>(batch, sp, al, be, part,
+                                                                             partial_stride);
     else if (t.bm == 32)
-      zgemm_dmma_kernel<FORM, 32, 128, 1><<<grid, kGemmThreads, 0, stream>>>(batch, sp, alpha, beta, part,
-                                                                           partial_stride);
-    else
-      zgemm_dmma_kernel<FORM, 64, 64, 2><<<grid, kGemmThreads, 0, stream>>>(batch, sp, alpha, beta, part,
-                                                                          partial_stride);
+      zgemm_dmma_kernel<T, FORM, 32, 128, 1><<<grid, kGemmThreads, 0, stream>>>(batch, sp, al, be, part,
+                                                                              partial_stride);
+    else if constexpr (std::is_same<T, double>::value)
+      zgemm_dmma_kernel<T, FORM, 64, 64, 2><<<grid, kGemmThreads, 0, stream>>>(batch, sp, al, be, part,
+                                                                             partial_stride);
     if (splits <= 1) return cudaGetLastError();
   } else {
     if (splits <= 1) {
