@@ -47,3 +47,28 @@ def test_si64_family_cells():
     assert np.all(np.abs(e) <= 0.01 + 1e-12)
     again, _ = make_cell(1000, "si64")
     np.testing.assert_array_equal(again.positions, a.positions)
+
+
+def test_dataset_shards_cover_every_seed_once_and_keep_seed_order(tmp_path, monkeypatch):
+    """generate() splits seeds into interleaved shards (one per worker process) and writes the
+    samples in seed order; here one worker and a stand-in for the cell convergence."""
+    from amaterasu_b200 import learned_pipeline as lp
+    seeds = list(range(1000, 1011))
+    shards = lp._shards(seeds, 4)
+    assert sorted(s for part in shards for s in part) == seeds
+    assert [len(p) for p in shards] == [3, 3, 3, 2]
+    assert lp._shards(seeds[:2], 4) == [[1000], [1001]]  # no empty shard (no idle process)
+
+    def fake_cell(seed, pseudo, **kw):
+        grid = np.full((2, 2, 2), float(seed), dtype=np.float32)
+        return dict(seed=seed, grid=[2, 2, 2], iterations=seed % 7, converged=True, free_energy=-1.0,
+                    seconds=0.5, n0=grid, nconv=grid + 1, strain=np.full(6, seed * 1e-6))
+
+    monkeypatch.setattr(lp, "run_cell", fake_cell)
+    monkeypatch.setattr(lp, "_pseudo", lambda: None)
+    order = [1004, 1001, 1003]
+    lp.generate(order, tmp_path / "d.npz")
+    data = np.load(tmp_path / "d.npz")
+    np.testing.assert_array_equal(data["seeds"], order)
+    np.testing.assert_array_equal(data["n0"][:, 0, 0, 0], order)
+    np.testing.assert_array_equal(data["iterations"], [s % 7 for s in order])
