@@ -219,7 +219,7 @@ __global__ void __launch_bounds__(kSmT) valid_prefix_kernel(uint8_t* __restrict_
     valid[t] = (t % cap) < count;
 }
 
-// valid[k][m + i] = keep[k][i] for i < nn: the rank test's verdict on the appended rows.
+// valid[k][m + i] = keep[k][i] for i < nn: the rank test's decision on the appended rows.
 __global__ void __launch_bounds__(kSmT) valid_append_kernel(uint8_t* __restrict__ valid, const uint8_t* __restrict__ keep,
                                                             int nk, int cap, int m, int nn) {
   for (int64_t t = blockIdx.x * (int64_t)kSmT + threadIdx.x; t < (int64_t)nk * nn; t += (int64_t)gridDim.x * kSmT) {
